@@ -1,0 +1,72 @@
+"""Regenerate the golden fixtures in this directory from the reference itself.
+
+Runs the reference's own sources (diskfft/src/hydro.hpp, kalnajs.hpp, diskmain.cpp,
+test_kalnajs.cpp), compiled unmodified against the project's FFTW shim by
+`make -C oracle ref` into oracle/_ref/, and stores their outputs:
+
+  ref_<case>.npz        fields from oracle/_ref/refdump: the standard-disk initial state,
+                        its potential and forces, the dt sequence, and the state after
+                        n steps of timestep -> potential -> forces -> step
+  test_kalnajs_ref.txt  stdout of the reference's known-answer test (FFT vs direct sum)
+  diskdisk_ref_<case>/  modes table + stdout of a short unmodified `diskdisk` run
+
+Needs the reference tree (only present where the fixtures are generated); the tests
+read only the committed outputs.  Usage: python tests/golden/make_golden.py
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import oracle as O  # noqa: E402
+
+# name: (Nu, Nphi, eps, selfgrav, amp, nsteps)
+CASES = {
+    "32x32_sg": (32, 32, 0.02, 1, 1e-3, 20),
+    "48x40_sg": (48, 40, 0.01, 1, 5e-2, 15),
+    "16x24_nosg": (16, 24, 0.02, 0, 5e-2, 30),
+    "64x64_strong": (64, 64, 0.005, 1, 0.2, 40),
+    "8x12_sg": (8, 12, 0.04, 1, 0.1, 25),
+    "24x27_odd": (24, 27, 0.02, 1, 0.1, 12),
+}
+
+DISKDISK = {
+    # name: argv of diskdisk (Nu Nphi eps tlim selfgrav amp nthreads)
+    "64_t1": ["64", "64", "0.01", "1.0", "1", "1e-3", "1"],
+}
+
+
+def main():
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", "ref"], check=True)
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    tmp = os.path.join(HERE, "_tmp")
+    os.makedirs(tmp, exist_ok=True)
+    for name, (Nu, Nphi, eps, sg, amp, n) in CASES.items():
+        out = os.path.join(tmp, name + ".bin")
+        subprocess.run([os.path.join(ref, "refdump"), str(Nu), str(Nphi), repr(eps), str(sg),
+                        repr(amp), str(n), out], check=True)
+        r = O.read_refdump(out)
+        np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), **{k: np.asarray(v) for k, v in r.items()})
+    res = subprocess.run([os.path.join(ref, "test_kalnajs_ref")], capture_output=True, text=True)
+    with open(os.path.join(HERE, "test_kalnajs_ref.txt"), "w") as f:
+        f.write(res.stdout)
+        f.write(f"exit={res.returncode}\n")
+    for name, argv in DISKDISK.items():
+        d = os.path.join(HERE, f"diskdisk_ref_{name}")
+        os.makedirs(d, exist_ok=True)
+        res = subprocess.run([os.path.join(ref, "diskdisk_ref")] + argv, capture_output=True, text=True,
+                             cwd=d, check=True)
+        with open(os.path.join(d, "stdout.txt"), "w") as f:
+            f.write(res.stdout)
+        with open(os.path.join(d, "argv.txt"), "w") as f:
+            f.write(" ".join(argv) + "\n")
+    shutil.rmtree(tmp)
+
+
+if __name__ == "__main__":
+    main()
