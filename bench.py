@@ -1,0 +1,315 @@
+"""Benchmark of the diskfft time step on B200: zone-updates/s (hydro + FFT gravity).
+
+One "step" is one time step of one disk: dt (device CFL reduction fused in the hydro
+epilogue), the Kalnajs gravity convolution and the fused hydro sweep.  At N GPUs every
+rank advances its own disk (independent disks, weak scaling) and `value` is the total
+zone-updates/s of the job, timed on the device as the max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
+                  [--size 1024] [--impl ours|reference]
+
+--impl reference times the reference's own CPU implementation (diskfft/src hydro.hpp +
+kalnajs.hpp compiled unmodified against the FFTW-API shim, oracle/_ref/refbench) on the
+host cores for the same workload; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "heavy-disks_b200"))
+
+METRIC = "zone-updates/s/GPU (hydro+FFT gravity), mixed vs FP64 plain at matched γ,Ω_p"
+UNIT = "zone-updates/s"
+REFBENCH = os.path.join(ROOT, "oracle", "_ref", "refbench")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"])
+    ap.add_argument("--size", type=int, default=1024)
+    ap.add_argument("--eps", type=float, default=0.005)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(a):
+    return {
+        "workload": f"single standard heavy disk {a.size}x{a.size} (log R x phi), gravity on a "
+                    f"{2 * a.size}x{a.size} zero-padded grid, eps={a.eps}, m=2 seed amp 1e-3, "
+                    "one time step = CFL dt + Kalnajs gravity + van-Leer MUSCL hydro",
+        "Nu": a.size, "Nphi": a.size, "eps": a.eps,
+    }
+
+
+# ---------------------------------------------------------------------------------
+# CPU reference (host cores)
+
+def run_refbench(size, eps, threads, warm, steps):
+    out = subprocess.run([REFBENCH, str(size), str(size), repr(eps), str(threads), str(warm), str(steps)],
+                         capture_output=True, text=True, check=True).stdout
+    return json.loads(out.strip().splitlines()[-1])
+
+
+def cpu_sample(size, eps, seconds=10.0):
+    """Bounded sample of the reference build: estimate the step time, then time ~`seconds`."""
+    threads = os.cpu_count() or 1
+    if not os.path.exists(REFBENCH):
+        return None
+    probe = run_refbench(size, eps, threads, 1, 2)
+    per = probe["seconds"] / 2
+    steps = max(3, min(2000, int(seconds / max(per, 1e-6))))
+    r = run_refbench(size, eps, threads, 1, steps)
+    return {"value": r["zone_updates_per_s"], "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{steps} steps of the {size}x{size} disk (eps {eps}) by the reference's DiskHydro + "
+                      f"KalnajsSolver compiled unmodified with the project FFTW-API shim (not FFTW), "
+                      f"{threads} OpenMP threads, wall clock"}
+
+
+def reference_arm(a, rank):
+    if rank != 0:
+        return
+    if not os.path.exists(REFBENCH):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/refbench not built"}))
+        return
+    threads = os.cpu_count() or 1
+    r = run_refbench(a.size, a.eps, threads, max(a.warmup, 1), a.steps)
+    v = r["zone_updates_per_s"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1e3 * r["seconds"] / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload(a),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{a.steps} timed steps after {max(a.warmup, 1)} warm-up, reference "
+                                   "sources compiled unmodified with the project FFTW-API shim"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, n in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def physical_gpu_index(local):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        if local < len(ids) and ids[local].isdigit():
+            return int(ids[local])
+    return local
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), float(pk["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 1590.0, "fallback"
+
+
+# ---------------------------------------------------------------------------------
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        reference_arm(a, rank)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import diskgpu as D
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    N = a.size
+    rng = np.random.default_rng(12345 + rank)
+    phase0 = float(rng.uniform(0, np.pi))
+    disk = D.Disk(N, N, eps=a.eps, amp=1e-3, precision=a.precision, phase0=phase0, device=local)
+    disk.init_standard()
+    stream = torch.cuda.Stream()
+    disk.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(a.warmup, 3)):
+            flush.zero_()
+            disk.run_steps(1, 0.3, sync=False)
+        torch.cuda.synchronize()
+
+        # ---- timed region: K steps, L2 flushed (untimed) before each ----
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+        disk.profile(True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(physical_gpu_index(local)) as clk:
+            for k in range(a.steps):
+                flush.zero_()
+                ev[k][0].record(stream)
+                disk.run_steps(1, 0.3, sync=False)
+                ev[k][1].record(stream)
+            torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        prof = disk.profile_read()
+        disk.profile(False)
+        ms = sum(s.elapsed_time(e) for s, e in ev)
+    t_dev = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
+    ms_max = float(t_dev.item())
+    disk.run_steps(0, 0.3, sync=True)  # surfaces any device-side error of the timed steps
+    zones = N * N
+    value = world * zones * a.steps / (ms_max * 1e-3)
+
+    # ---- roofline of the fused hydro kernel (HBM bound) and the gravity ----
+    hbm_peak, tc_peak, peak_kind = measured_peaks()
+    word = 8 if a.precision == "fp64" else 4
+    hyd_ms, hyd_n = prof["hydro"]
+    grav_ms, grav_n = prof["gravity"]
+    hyd_bytes = 7 * word * zones  # read Sigma, vR, vphi, Phi; write Sigma, vR, vphi
+    hyd_gbs = hyd_bytes / (hyd_ms / max(hyd_n, 1) * 1e-3) / 1e9 if hyd_n else None
+    roof_hydro = {"kernel": "fused hydro sweep", "bound": "hbm", "achieved": hyd_gbs, "peak": hbm_peak,
+                  "unit": "GB/s", "frac": (hyd_gbs / hbm_peak) if hyd_gbs else None, "traffic": None,
+                  "bytes_alg_per_launch": hyd_bytes, "ms_per_launch": hyd_ms / max(hyd_n, 1),
+                  "peak_kind": peak_kind}
+    share = {"hydro": hyd_ms / ms if ms else None, "gravity": grav_ms / ms if ms else None}
+    roof = roof_hydro
+    if a.precision == "fp64" and grav_n:
+        # plain path: the FFT passes are HBM bound; algorithmic bytes per launch =
+        # Sigma in (8 B/zone) + phi spectrum out/in/out/in (4 x 8 B/zone) + khat (16 B/zone) + Phi out (8)
+        g_bytes = (8 + 4 * 8 + 16 + 8) * zones
+        g_gbs = g_bytes / (grav_ms / grav_n * 1e-3) / 1e9
+        roof_grav = {"kernel": "FP64 FFT gravity (3 passes)", "bound": "hbm", "achieved": g_gbs, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": g_gbs / hbm_peak, "traffic": None, "bytes_alg_per_launch": g_bytes,
+                     "ms_per_launch": grav_ms / grav_n, "peak_kind": peak_kind}
+        if grav_ms > hyd_ms:
+            roof = roof_grav
+        roof_all = [roof_hydro, roof_grav]
+    else:
+        roof_all = [roof_hydro]
+    launches_per_step = (4 if a.precision == "fp64" else 5) if True else 0
+
+    # ---- end to end through the C ABI on host buffers (pinned), every step ----
+    e2e = None
+    if a.e2e_steps > 0:
+        S, vR, vp = disk.get_state()
+        hs = [torch.from_numpy(x).pin_memory() for x in (S, vR, vp)]
+        arrs = [t.numpy() for t in hs]
+        with torch.cuda.stream(stream):
+            disk.step_host(*arrs)  # warm
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(a.e2e_steps):
+                disk.step_host(*arrs)
+            el = time.perf_counter() - t0
+        e2e = {"value": world * zones * a.e2e_steps / el if world == 1 else None, "unit": UNIT,
+               "h2d_bytes_per_step": 3 * 8 * zones, "d2h_bytes_per_step": 3 * 8 * zones + 8,
+               "how": "dg_step_host per step: FP64 host state (pinned) -> device, CFL dt, gravity, hydro, "
+                      "state -> host; wall clock"}
+        if world > 1:
+            t_e = torch.tensor([el], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
+            e2e["value"] = world * zones * a.e2e_steps / float(t_e.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_sample(N, a.eps)
+
+    if rank == 0:
+        cfg = workload(a)
+        cfg.update({"precision": a.precision, "l2": "flushed before every timed step (256 MiB device write, "
+                    "outside the timed events)", "stream": "caller stream via dg_set_stream",
+                    "phase_share": share})
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": max(a.warmup, 3), "ms_per_step": ms_max / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if a.precision == "fp64" else "f32 state + f64 basic state, split-bf16 DFT",
+            "data": "synthetic (standard heavy disk, seeded m=2 phase)", "config": cfg,
+            "roofline": roof, "roofline_all": roof_all, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches_per_step * a.steps, "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    disk.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,99 @@
+// Shared device-side definitions for the diskgpu kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dg {
+
+// Status bits raised on the device and read by the host at the end of a chunk.
+enum : int {
+  kStNonFinite = 1,   // dt or state became non-finite / non-positive
+  kStTimeout = 2,     // a bounded device wait gave up
+};
+
+constexpr int kMaxModes = 9;        // C_0 .. C_8 accumulated on device
+constexpr int kMaxRecords = 4096;   // device ring of mode records between host drains
+
+// Device-resident control block of one disk: the step loop runs without host sync.
+// Written only by the last CTA of the hydro kernel (and by host-side set-up).
+struct Ctl {
+  // --- host-written configuration (copied as one prefix, up to dtinv_bits) ---
+  double t;          // simulation time at the start of the next step (advanced by the device)
+  double tlim;       // loop stops when !(t < tlim)
+  double cfl;        // Courant number of the next dt (0.3 in diskmain.cpp:100)
+  double dt;         // dt of the next step
+  double tnext;      // next mode-record time (diskmain.cpp:93)
+  double dtout;      // record cadence (0.25)
+  double mD;         // disk mass used to normalise C_m
+  int fixed_dt;      // 1: dt was supplied by the host; no clip to tlim, no records
+  int mode_every_step;  // accumulate C_0..C_mmax every step (diagnostic mode)
+  int mmax;          // highest m accumulated in that mode
+  int pad0;
+  // --- device-maintained ---
+  unsigned long long dtinv_bits;   // running max of (sR + sphi) as ordered bits
+  unsigned int done_ctas;          // CTAs of the current launch that have finished
+  int status;                      // kSt* bits
+  long long step;                  // completed steps
+  int nrec;                        // records written since the last host drain
+  int pad1;
+  double modesum[2 * kMaxModes];   // re/im sums for the record being built
+  double last_modes[2 * kMaxModes];// the most recent per-step sums (mode_every_step)
+  double rec[kMaxRecords][4];      // t, |C0|, |C2|, arg C2
+};
+
+template <typename T> struct cplx_of;
+template <> struct cplx_of<double> { using type = double2; };
+template <> struct cplx_of<float> { using type = float2; };
+
+template <typename V>
+__device__ __forceinline__ V cmul(V a, V b) {
+  V r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+
+// Ordered atomic max for non-negative doubles (NaN compares above +inf, so a NaN
+// propagates into the max and is caught by the non-finite check).
+__device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double v) {
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide max that keeps NaN (fmax drops NaN, so NaN is tracked separately).
+template <int NT>
+__device__ __forceinline__ double block_max_nan(double v, double *red) {
+  bool bad = !(v == v);
+  v = bad ? 0.0 : v;
+  v = warp_max(v);
+  unsigned anybad = __any_sync(0xffffffffu, bad);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = anybad ? __longlong_as_double(0x7ff8000000000000ll) : v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+    r = red[0];
+    for (int k = 1; k < NT / 32; ++k) {
+      double x = red[k];
+      if (!(x == x) || !(r == r)) r = __longlong_as_double(0x7ff8000000000000ll);
+      else r = fmax(r, x);
+    }
+  }
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+}  // namespace dg

@@ -1,0 +1,158 @@
+/* diskgpu.h — C ABI of the B200 (sm_100a) diskfft time step.
+ *
+ * The library advances a razor-thin barotropic self-gravitating disk on a log-polar
+ * grid: second-order van-Leer MUSCL transport plus Kalnajs softened log-spiral
+ * self-gravity.  It is a drop-in for the time step of oklo/heavy-disks' `diskdisk`
+ * (diskfft/src/diskmain.cpp, hydro.hpp, kalnajs.hpp).
+ *
+ * Conventions
+ *   - Host buffers are caller-owned, FP64, row-major with index i*Nphi + j:
+ *     i is the radial (log-spaced) cell, j the azimuthal cell (hydro.hpp:44).
+ *   - Every call returns an int status: DG_OK (0), or a negative DG_ERR_* code.
+ *     No exception crosses the ABI.  dg_last_error() gives a one-line reason.
+ *   - One handle owns one disk on one CUDA device and one stream.  A handle is not
+ *     thread-safe; different handles may be used from different threads.
+ *   - The state lives in device memory between calls; set/get copy it.
+ *
+ * Precision
+ *   DG_PREC_FP64   the plain method: FP64 state and FP64 FFT gravity.  Matches the
+ *                  reference's FFTW+OpenMP run to <= 1e-10 relative.
+ *   DG_PREC_MIXED  FP32 perturbation about an FP64 axisymmetric basic state; the
+ *                  gravity convolution runs as split-BF16 tensor-core (tcgen05) DFT
+ *                  products with FP32 accumulation.
+ */
+#ifndef DISKGPU_H
+#define DISKGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DG_ABI_VERSION 1
+
+/* status codes */
+#define DG_OK 0
+#define DG_ERR_INVALID (-1)     /* invalid argument or NULL pointer */
+#define DG_ERR_CUDA (-2)        /* CUDA runtime error (message in dg_last_error) */
+#define DG_ERR_NONFINITE (-3)   /* state or dt became non-finite / non-positive */
+#define DG_ERR_UNSUPPORTED (-4) /* grid size or option not supported */
+#define DG_ERR_NOMEM (-5)       /* device or host allocation failed */
+#define DG_ERR_TIMEOUT (-6)     /* a bounded device wait gave up */
+#define DG_ERR_STATE (-7)       /* call out of order (e.g. step before any state is set) */
+
+#define DG_PREC_FP64 0
+#define DG_PREC_MIXED 1
+
+/* Physical and numerical parameters.  dg_params_default() fills the reference's
+ * standard heavy disk and CLI defaults (diskmain.cpp:17-29). */
+typedef struct dg_params {
+  int Nu, Nphi;          /* radial and azimuthal cells (argv[1], argv[2]) */
+  double Rin, Rout;      /* grid radii (0.25, 1.0) */
+  double Kpoly;          /* P = K Sigma^gamma (0.25) */
+  double gamma_gas;      /* (2.0) */
+  double gmstar;         /* G M_* of the central star (0.6) */
+  double G;              /* gravitational constant of the disk (1.0) */
+  double eps;            /* scale-free Kalnajs softening (argv[3], 0.02) */
+  int selfgrav;          /* 1: disk self-gravity on (argv[5]) */
+  double amp;            /* m=2 seed amplitude (argv[6], 1e-3) */
+  double phase0;         /* seed phase: Sigma0 (1 + amp cos 2(phi - phase0)); 0 = reference */
+  double R0, w2, S0;     /* Gaussian disk Sigma0 = S0 exp(-(R-R0)^2/w2) (0.45, 0.05, 0.372) */
+  int precision;         /* DG_PREC_FP64 or DG_PREC_MIXED */
+  int device;            /* CUDA device ordinal; -1 = the calling thread's current device */
+} dg_params;
+
+/* One row of the mode table: diskmain.cpp:93-97 prints t, |C0|, |C2|, arg(C2). */
+typedef struct dg_record {
+  double t;
+  double c0;    /* |C0| */
+  double c2;    /* |C2| */
+  double arg2;  /* arg(C2) = atan2(Im, Re) */
+} dg_record;
+
+typedef struct dg_handle dg_handle;
+
+/* Fill *p with the reference defaults (diskmain.cpp:17-29). */
+int dg_params_default(dg_params *p);
+
+/* Create a disk (DiskHydro ctor hydro.hpp:28-43 + KalnajsSolver ctor kalnajs.hpp:25-42:
+ * grid, device buffers, Green's-function table khat built once in FP64). */
+int dg_create(const dg_params *p, dg_handle **out);
+/* Release every device and host resource of the handle (NULL is a no-op). */
+void dg_destroy(dg_handle *h);
+/* Reason for the last non-zero status of this handle ("" if none). */
+const char *dg_last_error(const dg_handle *h);
+/* Static text for a status code. */
+const char *dg_status_string(int status);
+
+/* Grid: R (Nu), Rf (Nu+1), Vol (Nu) exactly as hydro.hpp:31-38.  Any pointer may be NULL. */
+int dg_grid(const dg_handle *h, double *R, double *Rf, double *Vol);
+
+/* Standard initial condition: self-gravitating equilibrium + m=2 seed (diskmain.cpp:34-63). */
+int dg_init_standard(dg_handle *h);
+/* Replace / read the state (DiskHydro::Sig, vR, vp; hydro.hpp:24). */
+int dg_set_state(dg_handle *h, const double *Sig, const double *vR, const double *vp);
+int dg_get_state(dg_handle *h, double *Sig, double *vR, double *vp);
+
+/* DiskHydro::timestep(cfl) (hydro.hpp:48-61): dt = cfl / max_ij (sR + sphi). */
+int dg_timestep(dg_handle *h, double cfl, double *dt);
+/* One step with the disk's own self-gravity when selfgrav is on: the body of
+ * diskmain.cpp:102-108 = potential -> forces -> DiskHydro::step(dt, gR, gp). */
+int dg_step(dg_handle *h, double dt);
+/* DiskHydro::step(dt, gR, gp) (hydro.hpp:63-70) with caller forces; gR and gp may both
+ * be NULL (no self-gravity, hydro.hpp:86-88). */
+int dg_step_forces(dg_handle *h, double dt, const double *gR, const double *gp);
+
+/* KalnajsSolver::potential (kalnajs.hpp:48-63) of a caller surface density. */
+int dg_potential(dg_handle *h, const double *Sig, double *Phi);
+/* KalnajsSolver::forces (kalnajs.hpp:65-80). */
+int dg_forces(dg_handle *h, const double *Phi, double *gR, double *gp);
+
+/* Disk mass m_D = sum Sigma dA of the current state (diskmain.cpp:66-70). */
+int dg_disk_mass(dg_handle *h, double *mD);
+/* Fourier amplitudes C_m = sum Sigma e^{-i m phi} dA / m_D for m = 0..mmax of the current
+ * state (diskmain.cpp:72-84, normalised by the m_D fixed at dg_init_standard / dg_set_state).
+ * re_im receives 2*(mmax+1) doubles: Re C_0, Im C_0, Re C_1, ... */
+int dg_modes(dg_handle *h, int mmax, double *re_im);
+/* FP64 global sums: mass = sum Sigma dA, angmom = sum Sigma vphi R dA. */
+int dg_conserved(dg_handle *h, double *mass, double *angmom);
+
+/* The time loop of diskmain.cpp:88-110 run on the device: repeat
+ * { record modes every dtout; dt = timestep(cfl); clip to tlim; gravity; step } while t < tlim,
+ * with no host synchronisation inside a chunk of steps.  Records are written to rec
+ * (up to max_rec); *n_rec, *t and *nsteps receive the counts and final time. */
+int dg_advance(dg_handle *h, double tlim, double cfl, double dtout, dg_record *rec, int max_rec,
+               int *n_rec, double *t, long long *nsteps);
+/* Simulation time and step count of the handle. */
+int dg_time(dg_handle *h, double *t, long long *nsteps);
+
+/* ---- GPU-side extensions (no counterpart in the CPU reference) ---- */
+
+/* Run subsequent work of this handle on the caller's CUDA stream (a cudaStream_t passed
+ * as void*; NULL restores the handle's own stream).  The caller keeps ownership. */
+int dg_set_stream(dg_handle *h, void *stream);
+/* Enqueue nsteps device-resident steps: dt = cfl / max(sR + sphi) is derived on the device
+ * from the state each step produces (no tlim clip, no records, no host synchronisation).
+ * With sync = 0 the call returns once the work is queued; a device-side error then shows
+ * up at the next synchronising call. */
+int dg_run_steps(dg_handle *h, int nsteps, double cfl, int sync);
+/* One reference-style step on caller host buffers, in place: upload (Sig, vR, vp), then
+ * timestep(cfl) -> potential -> forces -> step as diskmain.cpp:100-105, and download the
+ * new state; *dt receives the dt used.  This is DiskHydro::step on host vectors. */
+int dg_step_host(dg_handle *h, double cfl, double *Sig, double *vR, double *vp, double *dt);
+
+/* Per-phase device timing with CUDA events on the handle's stream. */
+#define DG_PROF_HYDRO 0   /* fused hydro kernel */
+#define DG_PROF_GRAVITY 1 /* whole gravity convolution */
+#define DG_PROF_CFL 2     /* standalone CFL reductions */
+#define DG_PROF_N 3
+int dg_profile_enable(dg_handle *h, int on);
+/* Accumulated milliseconds and launch counts per phase since the last read (resets). */
+int dg_profile_read(dg_handle *h, double *ms, long long *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DISKGPU_H */
