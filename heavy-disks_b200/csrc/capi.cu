@@ -559,7 +559,7 @@ int dg_potential(dg_handle *h, const double *Sig, double *Phi) {
   DG_CK(cudaSetDevice(h->dev));
   const size_t n = (size_t)h->p.Nu * h->p.Nphi;
   DG_CK(cudaMemcpyAsync(h->gA, Sig, n * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  int rc = h->potential64(h->gA, h->gB);
+  int rc = (h->p.precision == DG_PREC_MIXED) ? h->mixed_potential(h->gA, h->gB) : h->potential64(h->gA, h->gB);
   if (rc) return rc;
   DG_CK(cudaMemcpyAsync(Phi, h->gB, n * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   DG_CK(cudaStreamSynchronize(h->st));
@@ -721,7 +721,9 @@ int dg_step_host(dg_handle *h, double cfl, double *Sig, double *vR, double *vp, 
   if (!h->have_state) return h->fail(DG_ERR_STATE, "dg_step_host", "no basic state: call dg_set_state or dg_init_standard once");
   { int rc0 = h->sync_from_device(); if (rc0) return rc0; }
   DG_CK(cudaSetDevice(h->dev));
+  h->in_step_host = true;
   int rc = h->upload_state(Sig, vR, vp);
+  h->in_step_host = false;
   if (rc) return rc;
   rc = h->set_ctl_fields(h->t, INFINITY, cfl, 0.0, INFINITY, 1.0, 1);
   if (rc) return rc;

@@ -92,4 +92,7 @@ struct dg_handle {
   int mixed_conserved_launch(double *out2);
   int mixed_upload_state(const double *Sig, const double *vR, const double *vp);
   int mixed_download_state(double *Sig, double *vR, double *vp);
+  int mixed_gravity();
+  int mixed_potential(const double *dSig, double *dOut);
+  bool in_step_host = false;  // upload from dg_step_host keeps the mixed basic state
 };

@@ -1,15 +1,899 @@
-// Mixed-precision path: placeholder until the FP32-perturbation kernels land.
+// Mixed-precision path: FP32 perturbation state about an FP64 axisymmetric basic state,
+// gravity of the perturbation as a split-BF16 tensor-core DFT (four tcgen05 GEMMs).
+//
+// Gravity (kalnajs.hpp:48-63 restated as dense real DFT contractions; s = R^{3/2} sigma):
+//   G1  X[c][i]  = sum_j Fphi[c][j] s[i][j]     phi DFT, c in [0, Nphi): Re m=0..Nphi/2,
+//                                               Im m=1..ceil(Nphi/2)-1 (the other Im are 0)
+//   G2  W[c][p]  = KW[c][p] sum_i Cu[p][i] X[c][i]
+//                                               u DFT on 2 Nu rows (cos p=0..Nu, sin p=1..Nu-1)
+//                                               times (w_p / M) khat(p, m(c)) (khat is real and
+//                                               even in p, so cos and sin rows decouple)
+//   G3  Z[i][c]  = sum_p Cu[p][i] W[c][p]       inverse u DFT (only the Nu physical rows)
+//   G4  dPhi[i][j] = (-G du dphi / sqrt(R_i)) sum_c Z[i][c] Gphi[j][c]   inverse phi DFT
+// Each GEMM's epilogue writes the next GEMM's operand as a BF16 (hi, lo) pair in the
+// K-major layout it needs; the hydro kernel writes s for G1 and reads dPhi.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include <cudaTypedefs.h>
+
 #include "engine.h"
+#include "hydro32.cuh"
+#include "tc_gemm.cuh"
+#include "step_ctl.cuh"
 
-struct MixedState {};
+using namespace dg;
 
-#define MX_UNSUPPORTED return fail(DG_ERR_UNSUPPORTED, "mixed precision", "not built yet")
-int dg_handle::mixed_init() { MX_UNSUPPORTED; }
-void dg_handle::mixed_release() {}
-int dg_handle::mixed_enqueue_step() { MX_UNSUPPORTED; }
-int dg_handle::mixed_enqueue_step_forces(const double *, const double *) { MX_UNSUPPORTED; }
-int dg_handle::mixed_cfl_launch(int, int) { MX_UNSUPPORTED; }
-int dg_handle::mixed_modes_launch(int, double *) { MX_UNSUPPORTED; }
-int dg_handle::mixed_conserved_launch(double *) { MX_UNSUPPORTED; }
-int dg_handle::mixed_upload_state(const double *, const double *, const double *) { MX_UNSUPPORTED; }
-int dg_handle::mixed_download_state(double *, double *, double *) { MX_UNSUPPORTED; }
+namespace {
+
+struct SplitBuf {
+  __nv_bfloat16 *hi = nullptr, *lo = nullptr;
+};
+
+}  // namespace
+
+struct MixedState {
+  int Nu = 0, Nphi = 0;
+  // per-row / per-face tables
+  float *rowbuf = nullptr;    // packed FP32 row and face arrays
+  double *rowbufd = nullptr;  // packed FP64 row arrays
+  Rows32 rows{};
+  std::vector<double> S0, V0, g0;  // FP64 basic state (host)
+  // state ping-pong
+  float *sig[2] = {nullptr, nullptr}, *u[2] = {nullptr, nullptr}, *w[2] = {nullptr, nullptr};
+  // gravity operands and outputs
+  SplitBuf Sx, X1, Wt, Z, Fphi, Cu, CuT, Gphi;
+  float *KW = nullptr, *dPhi = nullptr, *phiscale = nullptr;
+  CUtensorMap mFphi[2], mSx[2], mX1[2], mCu[2], mCuT[2], mWt[2], mZ[2], mGphi[2];
+  bool tables_ready = false;
+};
+
+// ---------------------------------------------------------------------------------
+// TMA descriptors
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// K-major BF16 matrix [rows][cols] -> tiles of box_rows x 64 with 128-byte swizzle.
+static bool make_map(CUtensorMap *m, const void *base, uint64_t rows, uint64_t cols, uint32_t box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  if (((uintptr_t)base & 15) || (cols * 2) % 16) return false;
+  cuuint64_t gdim[2] = {cols, rows};
+  cuuint64_t gstride[1] = {cols * 2};
+  cuuint32_t box[2] = {64, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), gdim, gstride, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------------
+// DFT tables (built on the device in FP64, stored as BF16 pairs)
+
+__device__ __forceinline__ void put_split(SplitBuf b, size_t k, double x) {
+  float f = (float)x;
+  __nv_bfloat16 h = __float2bfloat16_rn(f);
+  b.hi[k] = h;
+  b.lo[k] = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+}
+
+// phi index c -> (m, is_imag)
+__device__ __forceinline__ void phi_mode(int c, int Nphi, int &m, bool &im) {
+  const int Nc = Nphi / 2 + 1;
+  if (c < Nc) { m = c; im = false; } else { m = c - Nc + 1; im = true; }
+}
+
+__global__ void k_tab_phi(SplitBuf F, SplitBuf Gt, int N) {
+  const size_t n = (size_t)N * N;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int a = (int)(k / N), b = (int)(k % N);
+    // F[c = a][j = b]
+    {
+      int m; bool im;
+      phi_mode(a, N, m, im);
+      long long r = ((long long)m * b) % N;
+      double sn, cs;
+      sincospi(2.0 * (double)r / N, &sn, &cs);
+      put_split(F, k, im ? -sn : cs);
+    }
+    // Gt[j = a][c = b]: inverse real DFT weights (1/N, doubled off the self-conjugate bins)
+    {
+      int m; bool im;
+      phi_mode(b, N, m, im);
+      long long r = ((long long)m * a) % N;
+      double sn, cs;
+      sincospi(2.0 * (double)r / N, &sn, &cs);
+      double wgt = (m == 0 || (N % 2 == 0 && m == N / 2)) ? 1.0 : 2.0;
+      put_split(Gt, k, (im ? -sn : cs) * wgt / N);
+    }
+  }
+}
+
+// Cu[p][i] (2Nu x Nu): p <= Nu cos(2 pi p i / M), p > Nu sin(2 pi (p - Nu) i / M); CuT = Cu^T
+__global__ void k_tab_u(SplitBuf Cu, SplitBuf CuT, int Nu) {
+  const int M = 2 * Nu;
+  const size_t n = (size_t)M * Nu;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int p = (int)(k / Nu), i = (int)(k % Nu);
+    bool sn_row = p > Nu;
+    int pp = sn_row ? p - Nu : p;
+    long long r = ((long long)pp * i) % M;
+    double sn, cs;
+    sincospi(2.0 * (double)r / M, &sn, &cs);
+    double v = sn_row ? sn : cs;
+    put_split(Cu, k, v);
+    put_split(CuT, (size_t)i * M + p, v);
+  }
+}
+
+// KW[c][p] = (w_p / M) Re khat(p, m(c)); khat is the FP64 r2c table [m][0..M)
+__global__ void k_tab_kw(float *KW, const double2 *khat, int Nu, int Nphi) {
+  const int M = 2 * Nu;
+  const size_t n = (size_t)Nphi * M;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int c = (int)(k / M), p = (int)(k % M);
+    int m; bool im;
+    phi_mode(c, Nphi, m, im);
+    int pp = p > Nu ? p - Nu : p;
+    double wgt = (p == 0 || p == Nu) ? 1.0 : 2.0;
+    KW[k] = (float)(wgt / M * khat[(size_t)m * M + pp].x);
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// state conversion (FP64 full fields <-> basic state + FP32 perturbation)
+
+__global__ void k_to_pert(const double *S, const double *vR, const double *vp, float *sig, float *u, float *w,
+                          SplitBuf Sx, Rows32 g) {
+  const size_t n = (size_t)g.Nu * g.Nphi;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k / g.Nphi);
+    float s = (float)(S[k] - g.S0d[i]);
+    sig[k] = s;
+    u[k] = (float)vR[k];
+    w[k] = (float)(vp[k] - g.V0d[i]);
+    float x = g.R32[i] * s;
+    __nv_bfloat16 h = __float2bfloat16_rn(x);
+    Sx.hi[k] = h;
+    Sx.lo[k] = __float2bfloat16_rn(x - __bfloat162float(h));
+  }
+}
+
+__global__ void k_from_pert(const float *sig, const float *u, const float *w, double *S, double *vR, double *vp,
+                            Rows32 g) {
+  const size_t n = (size_t)g.Nu * g.Nphi;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k / g.Nphi);
+    S[k] = g.S0d[i] + (double)sig[k];
+    vR[k] = (double)u[k];
+    vp[k] = g.V0d[i] + (double)w[k];
+  }
+}
+
+// s = R^{3/2} Sigma of a full FP64 field (dg_potential in mixed precision)
+__global__ void k_full_to_sx(const double *S, SplitBuf Sx, Rows32 g) {
+  const size_t n = (size_t)g.Nu * g.Nphi;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k / g.Nphi);
+    float x = (float)((double)g.R32[i] * S[k]);
+    __nv_bfloat16 h = __float2bfloat16_rn(x);
+    Sx.hi[k] = h;
+    Sx.lo[k] = __float2bfloat16_rn(x - __bfloat162float(h));
+  }
+}
+
+// s = R^{3/2} sigma of the current perturbation (the G1 operand)
+__global__ void k_sig_to_sx(const float *sig, SplitBuf Sx, Rows32 g) {
+  const size_t n = (size_t)g.Nu * g.Nphi;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k / g.Nphi);
+    float x = g.R32[i] * sig[k];
+    __nv_bfloat16 h = __float2bfloat16_rn(x);
+    Sx.hi[k] = h;
+    Sx.lo[k] = __float2bfloat16_rn(x - __bfloat162float(h));
+  }
+}
+
+__global__ void k_f32_to_f64(const float *a, double *b, size_t n) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    b[k] = (double)a[k];
+}
+
+// ---------------------------------------------------------------------------------
+// fused hydro step on the perturbation
+
+__global__ void __launch_bounds__(kHydro32Threads) k_hydro32(const float *__restrict__ sig, const float *__restrict__ uu,
+                                                              const float *__restrict__ ww, const float *__restrict__ Phi,
+                                                              const double *__restrict__ gRin,
+                                                              const double *__restrict__ gpin, int force_mode,
+                                                              float *__restrict__ so, float *__restrict__ uo,
+                                                              float *__restrict__ wo, SplitBuf Sx, Ctl *ctl, Rows32 g) {
+  __shared__ float sS[kLI32][kLJ32], sU[kLI32][kLJ32], sW[kLI32][kLJ32], sP[kLI32][kLJ32], sPh[kLI32][kLJ32];
+  __shared__ float sU1[kSI32][kSJ32], sW1[kSI32][kSJ32];
+  __shared__ float fF[kTI32 + 1][kSJ32], fFR[kTI32 + 1][kSJ32], fGA[kTI32 + 1][kSJ32], fGB[kTI32 + 1][kSJ32];
+  __shared__ float pF[3 * kTI32][kTJ32 + 1];
+  __shared__ double red[kHydro32Threads / 32];
+  float(*s2S)[kLJ32] = sP;  // transportR outputs reuse dead tiles
+  float(*s2U)[kLJ32] = sU;
+  float(*s2W)[kLJ32] = sW;
+
+  const int Nu = g.Nu, Nphi = g.Nphi;
+  const int i0 = blockIdx.y * kTI32, j0 = blockIdx.x * kTJ32;
+  const int tid = threadIdx.x;
+  const StepInfo si = read_step_info(ctl, true);
+  const int nmodes = si.nmodes;
+  const float dt = (float)si.dt;
+  double msum[2 * kMaxModes];
+#pragma unroll
+  for (int q = 0; q < 2 * kMaxModes; ++q) msum[q] = 0.0;
+  double lmax = 0.0;
+  bool bad = false;
+
+  if (!si.active) {
+    for (int c = tid; c < kTI32 * kTJ32; c += kHydro32Threads) {
+      int i = i0 + c / kTJ32, j = j0 + c % kTJ32;
+      if (i < Nu && j < Nphi) {
+        size_t k = (size_t)i * Nphi + j;
+        so[k] = sig[k]; uo[k] = uu[k]; wo[k] = ww[k];
+        lmax = fmax(lmax, (double)cfl_rate32(g, i, sig[k], uu[k], ww[k]));
+      }
+    }
+    finish_launch<kHydro32Threads>(ctl, si, lmax, msum, red);
+    return;
+  }
+
+  // ---- load halo region ----
+  for (int c = tid; c < kLI32 * kLJ32; c += kHydro32Threads) {
+    int li = c / kLJ32, lj = c % kLJ32;
+    int i = i0 - kH32 + li;
+    int j = j0 - kH32 + lj;
+    j = ((j % Nphi) + Nphi) % Nphi;
+    float s = 0.f, a = 0.f, b = 0.f, ph = 0.f, dp = 0.f;
+    if (i >= 0 && i < Nu) {
+      size_t k = (size_t)i * Nphi + j;
+      s = sig[k]; a = uu[k]; b = ww[k];
+      if (force_mode == kForcePhi) ph = Phi[k];
+      dp = dpres32(g, i, s);
+    }
+    sS[li][lj] = s; sU[li][lj] = a; sW[li][lj] = b; sPh[li][lj] = ph; sP[li][lj] = dp;
+  }
+  __syncthreads();
+
+  // ---- source on rows i0-2 .. i0+TI+1 ----
+  for (int c = tid; c < kSI32 * kSJ32; c += kHydro32Threads) {
+    int si_ = c / kSJ32, sj = c % kSJ32;
+    int i = i0 - 2 + si_;
+    int li = si_ + 1, lj = sj + 1;
+    float nu = 0.f, nw = 0.f;
+    if (i >= 0 && i < Nu) {
+      int im = i - 1 > 0 ? i - 1 : 0, ip = i + 1 < Nu - 1 ? i + 1 : Nu - 1;
+      int lim = li + (im - i), lip = li + (ip - i);
+      const float sg = sS[li][lj];
+      const float s = g.S0[i] + sg;
+      const float ddP = (sP[lip][lj] - sP[lim][lj]) * g.invdRc[i];
+      const float dPdphi = (sP[li][lj + 1] - sP[li][lj - 1]) * g.inv2dphi;
+      float dgR = 0.f, dgp = 0.f;
+      if (force_mode == kForcePhi) {
+        float dPhidu;
+        if (i == 0) dPhidu = (sPh[li + 1][lj] - sPh[li][lj]) * g.invdu;
+        else if (i == Nu - 1) dPhidu = (sPh[li][lj] - sPh[li - 1][lj]) * g.invdu;
+        else dPhidu = (sPh[li + 1][lj] - sPh[li - 1][lj]) * g.inv2du;
+        dgR = -dPhidu * g.invR[i];
+        dgp = -(sPh[li][lj + 1] - sPh[li][lj - 1]) * g.inv2dphi * g.invR[i];
+      } else if (force_mode == kForceArrays) {
+        int j = ((j0 - 2 + sj) % Nphi + Nphi) % Nphi;
+        size_t k = (size_t)i * Nphi + j;
+        // caller forces are full fields: their axisymmetric part is in a0 only when they
+        // equal the basic-state gravity, so apply them in full and drop g0 from a0
+        dgR = (float)gRin[k];
+        dgp = (float)gpin[k];
+      }
+      const float uc = sU[li][lj], wc = sW[li][lj];
+      const float V = g.V0[i];
+      const float aR = g.a0[i] + (g.dP0dR[i] * sg * g.invS0[i] - ddP) / s + dgR + (2.f * V + wc) * wc * g.invR[i];
+      const float ap = -dPdphi / (s * g.R[i]) + dgp - uc * (V + wc) * g.invR[i];
+      nu = uc + dt * aR;
+      nw = wc + dt * ap;
+    }
+    sU1[si_][sj] = nu;
+    sW1[si_][sj] = nw;
+  }
+  __syncthreads();
+
+  // ---- transportR fluxes at faces f = i0 .. i0+TI ----
+  auto SG = [&](int i, int sj) { return sS[i - (i0 - 2) + 1][sj + 1]; };
+  auto U1 = [&](int i, int sj) { return sU1[i - (i0 - 2)][sj]; };
+  auto W1 = [&](int i, int sj) { return sW1[i - (i0 - 2)][sj]; };
+  for (int c = tid; c < (kTI32 + 1) * kSJ32; c += kHydro32Threads) {
+    int fi = c / kSJ32, sj = c % kSJ32;
+    int f = i0 + fi;
+    float F = 0.f, FR = 0.f, GA = 0.f, GB = 0.f;
+    if (f >= 1 && f <= Nu - 1) {
+      const float vf = 0.5f * (U1(f - 1, sj) + U1(f, sj));
+      int cc;
+      float hf;
+      if (vf > 0.f) { cc = f - 1; hf = 0.5f * (1.f - vf * dt / g.dRl[f]); }
+      else { cc = f; hf = -0.5f * (1.f + vf * dt / g.dRr[f]); }
+      float kS = 0.f, kU = 0.f, kV = 0.f;
+      if (cc > 0 && cc < Nu - 1) {
+        kS = vanleer32(g.dS0[cc + 1] + (SG(cc + 1, sj) - SG(cc, sj)), g.dS0[cc] + (SG(cc, sj) - SG(cc - 1, sj)));
+        kU = vanleer32(U1(cc + 1, sj) - U1(cc, sj), U1(cc, sj) - U1(cc - 1, sj));
+        kV = vanleer32(g.dV[cc + 1] + (W1(cc + 1, sj) - W1(cc, sj)), g.dV[cc] + (W1(cc, sj) - W1(cc - 1, sj)));
+      }
+      const float Sf = g.S0[cc] + SG(cc, sj) + hf * kS;
+      const float uf = U1(cc, sj) + hf * kU;
+      const float Df = (cc == f ? g.dV[f] : 0.f) + W1(cc, sj) + hf * kV;  // vphi_f - V0(f-1)
+      F = vf * Sf * g.Af[f];
+      FR = F * uf;
+      GA = F * Df;
+      GB = F * (Df - g.dV[f]);
+    }
+    fF[fi][sj] = F; fFR[fi][sj] = FR; fGA[fi][sj] = GA; fGB[fi][sj] = GB;
+  }
+  __syncthreads();
+
+  // ---- transportR gather on rows i0 .. i0+TI-1 ----
+  for (int c = tid; c < kTI32 * kSJ32; c += kHydro32Threads) {
+    int ri = c / kSJ32, sj = c % kSJ32;
+    int i = i0 + ri;
+    float ns = 0.f, a = 0.f, b = 0.f;
+    if (i < Nu) {
+      const float sg = SG(i, sj), u1 = U1(i, sj), w1 = W1(i, sj);
+      const float s = g.S0[i] + sg;
+      const float iv = g.invVol[i];
+      ns = sg + dt * (fF[ri][sj] - fF[ri + 1][sj]) * iv;
+      float s2 = g.S0[i] + ns;
+      float d = (s2 < 1e-10f) ? 1e-10f : s2;
+      a = (s * u1 + dt * (fFR[ri][sj] - fFR[ri + 1][sj]) * iv) / d;
+      b = (s * w1 + dt * (fGB[ri][sj] - fGA[ri + 1][sj]) * iv) / d;
+    }
+    s2S[ri][sj] = ns; s2U[ri][sj] = a; s2W[ri][sj] = b;
+  }
+  __syncthreads();
+
+  // ---- transportPhi fluxes: face pj = j-1/2 of cell j0+pj ----
+  for (int c = tid; c < kTI32 * (kTJ32 + 1); c += kHydro32Threads) {
+    int ri = c / (kTJ32 + 1), pj = c % (kTJ32 + 1);
+    int i = i0 + ri;
+    float Fm = 0.f, FR = 0.f, G = 0.f;
+    if (i < Nu) {
+      const int cm = pj + 1, cc = pj + 2;
+      const float V = g.V0[i];
+      const float dv = 0.5f * (s2W[ri][cm] + s2W[ri][cc]);
+      const float vf = V + dv;
+      const int up = (vf > 0.f) ? cm : cc;
+      const float hf = (vf > 0.f) ? 0.5f * (1.f - vf * dt / g.dl[i]) : -0.5f * (1.f + vf * dt / g.dl[i]);
+      const float kS = vanleer32(s2S[ri][up + 1] - s2S[ri][up], s2S[ri][up] - s2S[ri][up - 1]);
+      const float kU = vanleer32(s2U[ri][up + 1] - s2U[ri][up], s2U[ri][up] - s2U[ri][up - 1]);
+      const float kW = vanleer32(s2W[ri][up + 1] - s2W[ri][up], s2W[ri][up] - s2W[ri][up - 1]);
+      const float sf = s2S[ri][up] + hf * kS;
+      const float Sf = g.S0[i] + sf;
+      const float uf = s2U[ri][up] + hf * kU;
+      const float wf = s2W[ri][up] + hf * kW;
+      const float A = g.Aphi[i];
+      const float Ffull = vf * Sf * A;
+      Fm = A * (V * sf + dv * Sf);
+      FR = Ffull * uf;
+      G = Ffull * wf;
+    }
+    pF[ri][pj] = Fm; pF[kTI32 + ri][pj] = FR; pF[2 * kTI32 + ri][pj] = G;
+  }
+  __syncthreads();
+
+  // ---- transportPhi gather + floor + outputs + next-step CFL ----
+  for (int c = tid; c < kTI32 * kTJ32; c += kHydro32Threads) {
+    int ri = c / kTJ32, pj = c % kTJ32;
+    int i = i0 + ri, j = j0 + pj;
+    if (i < Nu && j < Nphi) {
+      const int cc = pj + 2;
+      const float sg2 = s2S[ri][cc], u2 = s2U[ri][cc], w2 = s2W[ri][cc];
+      const float iv = g.invVol[i];
+      const float S0 = g.S0[i];
+      const float s2 = S0 + sg2;
+      float sg3 = sg2 + dt * (pF[ri][pj] - pF[ri][pj + 1]) * iv;
+      const float s3 = S0 + sg3;
+      const float d = (s3 < 1e-10f) ? 1e-10f : s3;
+      const float u3 = (s2 * u2 + dt * (pF[kTI32 + ri][pj] - pF[kTI32 + ri][pj + 1]) * iv) / d;
+      const float w3 = (s2 * w2 + dt * (pF[2 * kTI32 + ri][pj] - pF[2 * kTI32 + ri][pj + 1]) * iv) / d;
+      if (s3 < 1e-10f) sg3 = 1e-10f - S0;  // floor (hydro.hpp:69)
+      const size_t k = (size_t)i * Nphi + j;
+      so[k] = sg3; uo[k] = u3; wo[k] = w3;
+      const float x = g.R32[i] * sg3;
+      const __nv_bfloat16 hx = __float2bfloat16_rn(x);
+      Sx.hi[k] = hx;
+      Sx.lo[k] = __float2bfloat16_rn(x - __bfloat162float(hx));
+      const float rate = cfl_rate32(g, i, sg3, u3, w3);
+      bad |= !(rate == rate) || !(u3 == u3) || !(w3 == w3);
+      lmax = fmax(lmax, (double)rate);
+      if (nmodes) {
+        const double sfull = g.S0d[i] + (double)sg3;
+        const double phi = (j + 0.5) * (double)g.dphi;
+        for (int m = 0; m < nmodes; ++m) {
+          double sn, cs;
+          sincos(m * phi, &sn, &cs);
+          msum[2 * m] += sfull * cs * g.dAd[i];
+          msum[2 * m + 1] -= sfull * sn * g.dAd[i];
+        }
+      }
+    }
+  }
+  if (bad) lmax = __longlong_as_double(0x7ff8000000000000ll);
+  finish_launch<kHydro32Threads>(ctl, si, lmax, msum, red);
+}
+
+// CFL (and optional mode sums) over the perturbation state
+__global__ void __launch_bounds__(256) k_cfl32(const float *sig, const float *uu, const float *ww, Ctl *ctl, Rows32 g,
+                                               int nmodes, int record) {
+  __shared__ double red[8];
+  double msum[2 * kMaxModes];
+#pragma unroll
+  for (int q = 0; q < 2 * kMaxModes; ++q) msum[q] = 0.0;
+  if (record && nmodes < 3) nmodes = 3;
+  double lmax = 0.0;
+  bool bad = false;
+  const size_t n = (size_t)g.Nu * g.Nphi;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k / g.Nphi), j = (int)(k % g.Nphi);
+    float r = cfl_rate32(g, i, sig[k], uu[k], ww[k]);
+    bad |= !(r == r);
+    lmax = fmax(lmax, (double)r);
+    if (nmodes) {
+      const double sfull = g.S0d[i] + (double)sig[k];
+      const double phi = (j + 0.5) * (double)g.dphi;
+      for (int m = 0; m < nmodes; ++m) {
+        double sn, cs;
+        sincos(m * phi, &sn, &cs);
+        msum[2 * m] += sfull * cs * g.dAd[i];
+        msum[2 * m + 1] -= sfull * sn * g.dAd[i];
+      }
+    }
+  }
+  if (bad) lmax = __longlong_as_double(0x7ff8000000000000ll);
+  StepInfo si;
+  si.t = ctl->t; si.dt = 0.0; si.tlim = ctl->tlim;
+  si.active = false; si.advance_t = false; si.record = record != 0; si.nmodes = nmodes;
+  finish_launch<256>(ctl, si, lmax, msum, red);
+}
+
+__global__ void __launch_bounds__(256) k_modes32(const float *sig, Rows32 g, int nmodes, double *out) {
+  __shared__ double red[8];
+  double msum[2 * kMaxModes];
+#pragma unroll
+  for (int q = 0; q < 2 * kMaxModes; ++q) msum[q] = 0.0;
+  const size_t n = (size_t)g.Nu * g.Nphi;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k / g.Nphi), j = (int)(k % g.Nphi);
+    const double sfull = g.S0d[i] + (double)sig[k];
+    const double phi = (j + 0.5) * (double)g.dphi;
+    for (int m = 0; m < nmodes; ++m) {
+      double sn, cs;
+      sincos(m * phi, &sn, &cs);
+      msum[2 * m] += sfull * cs * g.dAd[i];
+      msum[2 * m + 1] -= sfull * sn * g.dAd[i];
+    }
+  }
+  for (int q = 0; q < 2 * nmodes; ++q) {
+    double v = warp_sum(msum[q]);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < 8; ++w) s += red[w];
+      atomicAdd(&out[q], s);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_conserved32(const float *sig, const float *ww, Rows32 g, double *out) {
+  __shared__ double red[2][8];
+  double m = 0.0, L = 0.0;
+  const size_t n = (size_t)g.Nu * g.Nphi;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k / g.Nphi);
+    const double s = g.S0d[i] + (double)sig[k];
+    const double vp = g.V0d[i] + (double)ww[k];
+    m += s * g.dAd[i];
+    L += s * vp * g.Rd[i] * g.dAd[i];
+  }
+  m = warp_sum(m);
+  L = warp_sum(L);
+  if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = m; red[1][threadIdx.x >> 5] = L; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int w = 0; w < 8; ++w) { a += red[0][w]; b += red[1][w]; }
+    atomicAdd(&out[0], a);
+    atomicAdd(&out[1], b);
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// host side
+
+#define XK(call)                                                                    \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) return fail(DG_ERR_CUDA, #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+static int grid_for(size_t n) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  size_t b = (n + 255) / 256;
+  size_t cap = (size_t)sms * 8;
+  return (int)(b < cap ? b : cap);
+}
+
+template <typename T>
+static cudaError_t dalloc(T **p, size_t n) {
+  return cudaMalloc((void **)p, (n ? n : 1) * sizeof(T));
+}
+
+static cudaError_t alloc_split(SplitBuf &b, size_t n) {
+  cudaError_t e = dalloc(&b.hi, n);
+  if (e != cudaSuccess) return e;
+  return dalloc(&b.lo, n);
+}
+
+static void free_split(SplitBuf &b) {
+  if (b.hi) cudaFree(b.hi);
+  if (b.lo) cudaFree(b.lo);
+  b.hi = b.lo = nullptr;
+}
+
+int dg_handle::mixed_init() {
+  const int Nu = p.Nu, Nphi = p.Nphi;
+  if (Nu % tc::BM || Nphi % tc::BM) {
+    char b[160];
+    snprintf(b, sizeof b, "Nu=%d Nphi=%d: the tensor-core gravity needs multiples of %d", Nu, Nphi, tc::BM);
+    return fail(DG_ERR_UNSUPPORTED, "mixed precision", b);
+  }
+  if (!encode_fn()) return fail(DG_ERR_UNSUPPORTED, "mixed precision", "cuTensorMapEncodeTiled unavailable");
+  mx = new MixedState();
+  MixedState &X = *mx;
+  X.Nu = Nu;
+  X.Nphi = Nphi;
+  const size_t n = (size_t)Nu * Nphi;
+  for (int b = 0; b < 2; ++b) {
+    XK(dalloc(&X.sig[b], n)); XK(dalloc(&X.u[b], n)); XK(dalloc(&X.w[b], n));
+  }
+  XK(alloc_split(X.Sx, n)); XK(alloc_split(X.X1, n)); XK(alloc_split(X.Z, n));
+  XK(alloc_split(X.Wt, (size_t)Nphi * 2 * Nu));
+  XK(alloc_split(X.Fphi, (size_t)Nphi * Nphi)); XK(alloc_split(X.Gphi, (size_t)Nphi * Nphi));
+  XK(alloc_split(X.Cu, (size_t)2 * Nu * Nu)); XK(alloc_split(X.CuT, (size_t)2 * Nu * Nu));
+  XK(dalloc(&X.KW, (size_t)Nphi * 2 * Nu));
+  XK(dalloc(&X.dPhi, n));
+  XK(dalloc(&X.phiscale, Nu));
+  XK(dalloc(&X.rowbuf, (size_t)20 * (Nu + 1)));
+  XK(dalloc(&X.rowbufd, (size_t)4 * Nu));
+  // DFT tables
+  k_tab_phi<<<grid_for((size_t)Nphi * Nphi), 256, 0, st>>>(X.Fphi, X.Gphi, Nphi);
+  XK(cudaGetLastError());
+  k_tab_u<<<grid_for((size_t)2 * Nu * Nu), 256, 0, st>>>(X.Cu, X.CuT, Nu);
+  XK(cudaGetLastError());
+  k_tab_kw<<<grid_for((size_t)Nphi * 2 * Nu), 256, 0, st>>>(X.KW, Khat, Nu, Nphi);
+  XK(cudaGetLastError());
+  std::vector<float> ps(Nu);
+  for (int i = 0; i < Nu; ++i) ps[i] = (float)(-p.G * du * dphi / sqrtR[i]);
+  XK(cudaMemcpy(X.phiscale, ps.data(), Nu * sizeof(float), cudaMemcpyHostToDevice));
+  // tensor maps: A operands are read in 128-row boxes, B operands in 64-row boxes
+  bool okm = make_map(&X.mFphi[0], X.Fphi.hi, Nphi, Nphi, tc::BM) && make_map(&X.mFphi[1], X.Fphi.lo, Nphi, Nphi, tc::BM) &&
+             make_map(&X.mSx[0], X.Sx.hi, Nu, Nphi, tc::BN) && make_map(&X.mSx[1], X.Sx.lo, Nu, Nphi, tc::BN) &&
+             make_map(&X.mX1[0], X.X1.hi, Nphi, Nu, tc::BM) && make_map(&X.mX1[1], X.X1.lo, Nphi, Nu, tc::BM) &&
+             make_map(&X.mCu[0], X.Cu.hi, 2 * Nu, Nu, tc::BN) && make_map(&X.mCu[1], X.Cu.lo, 2 * Nu, Nu, tc::BN) &&
+             make_map(&X.mCuT[0], X.CuT.hi, Nu, 2 * Nu, tc::BM) && make_map(&X.mCuT[1], X.CuT.lo, Nu, 2 * Nu, tc::BM) &&
+             make_map(&X.mWt[0], X.Wt.hi, Nphi, 2 * Nu, tc::BN) && make_map(&X.mWt[1], X.Wt.lo, Nphi, 2 * Nu, tc::BN) &&
+             make_map(&X.mZ[0], X.Z.hi, Nu, Nphi, tc::BM) && make_map(&X.mZ[1], X.Z.lo, Nu, Nphi, tc::BM) &&
+             make_map(&X.mGphi[0], X.Gphi.hi, Nphi, Nphi, tc::BN) && make_map(&X.mGphi[1], X.Gphi.lo, Nphi, Nphi, tc::BN);
+  if (!okm) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed");
+  XK(cudaFuncSetAttribute(tc::k_gemm_split<tc::kEpiSplit>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)tc::kSmemBytes));
+  XK(cudaFuncSetAttribute(tc::k_gemm_split<tc::kEpiSplitScaled>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)tc::kSmemBytes));
+  XK(cudaFuncSetAttribute(tc::k_gemm_split<tc::kEpiRowScaleF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)tc::kSmemBytes));
+  XK(cudaStreamSynchronize(st));
+  X.tables_ready = true;
+  return DG_OK;
+}
+
+void dg_handle::mixed_release() {
+  if (!mx) return;
+  MixedState &X = *mx;
+  for (int b = 0; b < 2; ++b) {
+    if (X.sig[b]) cudaFree(X.sig[b]);
+    if (X.u[b]) cudaFree(X.u[b]);
+    if (X.w[b]) cudaFree(X.w[b]);
+  }
+  SplitBuf *bufs[] = {&X.Sx, &X.X1, &X.Wt, &X.Z, &X.Fphi, &X.Cu, &X.CuT, &X.Gphi};
+  for (SplitBuf *b : bufs) free_split(*b);
+  void *ptrs[] = {X.KW, X.dPhi, X.phiscale, X.rowbuf, X.rowbufd};
+  for (void *q : ptrs)
+    if (q) cudaFree(q);
+  delete mx;
+  mx = nullptr;
+}
+
+// Basic state and its per-row tables.  S0, V0 are the phi averages of the given state
+// (exactly the unperturbed profiles after dg_init_standard), g0 the phi-averaged radial
+// force of the basic state's own FP64 potential.
+static int build_basic(dg_handle *h, const double *Sig, const double *vp) {
+  MixedState &X = *h->mx;
+  const dg_params &p = h->p;
+  const int Nu = p.Nu, Nphi = p.Nphi;
+  X.S0.assign(Nu, 0.0);
+  X.V0.assign(Nu, 0.0);
+  X.g0.assign(Nu, 0.0);
+  if (h->basic_from_standard) {
+    X.S0 = h->std_sigma0;
+    X.V0 = h->std_vphi0;
+    X.g0 = h->std_gR0;
+  } else {
+    for (int i = 0; i < Nu; ++i) {
+      double a = 0, b = 0;
+      for (int j = 0; j < Nphi; ++j) { a += Sig[(size_t)i * Nphi + j]; b += vp[(size_t)i * Nphi + j]; }
+      X.S0[i] = a / Nphi;
+      X.V0[i] = b / Nphi;
+    }
+    if (p.selfgrav) {
+      const size_t n = (size_t)Nu * Nphi;
+      std::vector<double> axi(n), gR(n);
+      for (int i = 0; i < Nu; ++i)
+        for (int j = 0; j < Nphi; ++j) axi[(size_t)i * Nphi + j] = X.S0[i];
+      if (cudaMemcpyAsync(h->gA, axi.data(), n * sizeof(double), cudaMemcpyHostToDevice, h->st) != cudaSuccess)
+        return h->fail(DG_ERR_CUDA, "basic state", "upload");
+      int rc = h->potential64(h->gA, h->dPhi);
+      if (rc) return rc;
+      if (launch_forces64(h->dPhi, h->gA, h->gB, h->geom, h->st) != cudaSuccess ||
+          cudaMemcpyAsync(gR.data(), h->gA, n * sizeof(double), cudaMemcpyDeviceToHost, h->st) != cudaSuccess ||
+          cudaStreamSynchronize(h->st) != cudaSuccess)
+        return h->fail(DG_ERR_CUDA, "basic state", "gravity");
+      for (int i = 0; i < Nu; ++i) {
+        double s = 0;
+        for (int j = 0; j < Nphi; ++j) s += gR[(size_t)i * Nphi + j];
+        X.g0[i] = s / Nphi;
+      }
+    }
+  }
+  // FP64 row constants -> FP32 tables
+  const std::vector<double> &R = h->R, &Rf = h->Rf, &Vol = h->Vol;
+  const double K = p.Kpoly, gam = p.gamma_gas;
+  std::vector<double> P0(Nu), dP0dR(Nu), a0(Nu);
+  for (int i = 0; i < Nu; ++i) P0[i] = K * std::pow(X.S0[i], gam);
+  for (int i = 0; i < Nu; ++i) {
+    int im = i - 1 > 0 ? i - 1 : 0, ip = i + 1 < Nu - 1 ? i + 1 : Nu - 1;
+    dP0dR[i] = (P0[ip] - P0[im]) / (R[ip] - R[im]);
+    double gR = -p.gmstar / (R[i] * R[i]) + (p.selfgrav ? X.g0[i] : 0.0);
+    a0[i] = -dP0dR[i] / X.S0[i] + gR + X.V0[i] * X.V0[i] / R[i];
+  }
+  const int L = Nu + 1;
+  std::vector<float> rb((size_t)20 * L, 0.f);
+  auto col = [&](int k) { return rb.data() + (size_t)k * L; };
+  for (int i = 0; i < Nu; ++i) {
+    int im = i - 1 > 0 ? i - 1 : 0, ip = i + 1 < Nu - 1 ? i + 1 : Nu - 1;
+    col(0)[i] = (float)R[i];
+    col(1)[i] = (float)(1.0 / R[i]);
+    col(2)[i] = (float)(1.0 / (R[ip] - R[im]));
+    col(3)[i] = (float)dP0dR[i];
+    col(4)[i] = (float)X.S0[i];
+    col(5)[i] = (float)(1.0 / X.S0[i]);
+    col(6)[i] = (float)X.V0[i];
+    col(7)[i] = (float)a0[i];
+    col(8)[i] = (float)(Rf[i + 1] - Rf[i]);
+    col(9)[i] = (float)(R[i] * h->dphi);
+    col(10)[i] = (float)(Rf[i + 1] - Rf[i]);
+    col(11)[i] = (float)(1.0 / Vol[i]);
+    col(12)[i] = (float)h->R32[i];
+    col(13)[i] = (float)P0[i];
+  }
+  for (int f = 0; f <= Nu; ++f) {
+    col(14)[f] = (float)(Rf[f] * h->dphi);
+    col(15)[f] = (f >= 1) ? (float)(Rf[f] - Rf[f - 1]) : 0.f;
+    col(16)[f] = (f <= Nu - 1) ? (float)(Rf[f + 1] - Rf[f]) : 0.f;
+    col(17)[f] = (f >= 1 && f <= Nu - 1) ? (float)(X.V0[f] - X.V0[f - 1]) : 0.f;
+    col(18)[f] = (f >= 1 && f <= Nu - 1) ? (float)(X.S0[f] - X.S0[f - 1]) : 0.f;
+  }
+  std::vector<double> rd((size_t)4 * Nu);
+  for (int i = 0; i < Nu; ++i) {
+    rd[i] = X.S0[i];
+    rd[Nu + i] = X.V0[i];
+    rd[2 * Nu + i] = R[i];
+    rd[3 * Nu + i] = R[i] * (Rf[i + 1] - Rf[i]) * h->dphi;
+  }
+  if (cudaMemcpyAsync(X.rowbuf, rb.data(), rb.size() * sizeof(float), cudaMemcpyHostToDevice, h->st) != cudaSuccess ||
+      cudaMemcpyAsync(X.rowbufd, rd.data(), rd.size() * sizeof(double), cudaMemcpyHostToDevice, h->st) != cudaSuccess)
+    return h->fail(DG_ERR_CUDA, "basic state", "row tables");
+  Rows32 &g = X.rows;
+  float *b = X.rowbuf;
+  auto dc = [&](int k) { return (const float *)(b + (size_t)k * L); };
+  g.R = dc(0); g.invR = dc(1); g.invdRc = dc(2); g.dP0dR = dc(3); g.S0 = dc(4); g.invS0 = dc(5); g.V0 = dc(6);
+  g.a0 = dc(7); g.dR = dc(8); g.dl = dc(9); g.Aphi = dc(10); g.invVol = dc(11); g.R32 = dc(12); g.P0 = dc(13);
+  g.Af = dc(14); g.dRl = dc(15); g.dRr = dc(16); g.dV = dc(17); g.dS0 = dc(18);
+  g.S0d = X.rowbufd; g.V0d = X.rowbufd + Nu; g.Rd = X.rowbufd + 2 * Nu; g.dAd = X.rowbufd + 3 * Nu;
+  g.Nu = Nu; g.Nphi = Nphi;
+  g.dphi = (float)h->dphi; g.inv2dphi = (float)(1.0 / (2.0 * h->dphi));
+  g.invdu = (float)(1.0 / h->du); g.inv2du = (float)(1.0 / (2.0 * h->du));
+  g.Kpoly = (float)K; g.gamma = (float)gam; g.gmstar = (float)p.gmstar;
+  g.gamma2 = (gam == 2.0) ? 1 : 0;
+  return DG_OK;
+}
+
+int dg_handle::mixed_upload_state(const double *Sig, const double *vRh, const double *vph) {
+  MixedState &X = *mx;
+  const size_t n = (size_t)p.Nu * p.Nphi;
+  // a new basic state on dg_set_state / dg_init_standard; dg_step_host keeps the current one
+  if (!in_step_host) {
+    int rc = build_basic(this, Sig, vph);
+    if (rc) return rc;
+  }
+  XK(cudaMemcpyAsync(S[0], Sig, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  XK(cudaMemcpyAsync(VR[0], vRh, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  XK(cudaMemcpyAsync(VP[0], vph, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  k_to_pert<<<grid_for(n), 256, 0, st>>>(S[0], VR[0], VP[0], X.sig[cur], X.u[cur], X.w[cur], X.Sx, X.rows);
+  XK(cudaGetLastError());
+  return DG_OK;
+}
+
+int dg_handle::mixed_download_state(double *Sig, double *vRh, double *vph) {
+  MixedState &X = *mx;
+  const size_t n = (size_t)p.Nu * p.Nphi;
+  k_from_pert<<<grid_for(n), 256, 0, st>>>(X.sig[cur], X.u[cur], X.w[cur], S[0], VR[0], VP[0], X.rows);
+  XK(cudaGetLastError());
+  XK(cudaMemcpyAsync(Sig, S[0], n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  XK(cudaMemcpyAsync(vRh, VR[0], n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  XK(cudaMemcpyAsync(vph, VP[0], n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  XK(cudaStreamSynchronize(st));
+  return DG_OK;
+}
+
+template <int MODE>
+static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUtensorMap &Bh, const CUtensorMap &Bl,
+                        int M, int N, int K, const tc::GemmArgs &base, cudaStream_t st) {
+  tc::GemmArgs a = base;
+  a.M = M; a.N = N; a.K = K;
+  dim3 grid(N / tc::BN, M / tc::BM);
+  tc::k_gemm_split<MODE><<<grid, tc::kThreads, tc::kSmemBytes, st>>>(Ah, Al, Bh, Bl, a);
+  return cudaGetLastError();
+}
+
+// dPhi = gravity of s (the split operand in X.Sx)
+int dg_handle::mixed_gravity() {
+  MixedState &X = *mx;
+  const int Nu = p.Nu, Nphi = p.Nphi;
+  tc::GemmArgs a{};
+  a.status = &ctl->status;
+  // G1: X1[c][i] = Fphi[c][:] . Sx[i][:]
+  a.out_hi = X.X1.hi; a.out_lo = X.X1.lo; a.ldo = Nu;
+  XK(gemm<tc::kEpiSplit>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st));
+  // G2: Wt[c][p] = KW[c][p] * X1[c][:] . Cu[p][:]
+  a.out_hi = X.Wt.hi; a.out_lo = X.Wt.lo; a.ldo = 2 * Nu; a.table = X.KW;
+  XK(gemm<tc::kEpiSplitScaled>(X.mX1[0], X.mX1[1], X.mCu[0], X.mCu[1], Nphi, 2 * Nu, Nu, a, st));
+  // G3: Z[i][c] = CuT[i][:] . Wt[c][:]
+  a.out_hi = X.Z.hi; a.out_lo = X.Z.lo; a.ldo = Nphi; a.table = nullptr;
+  XK(gemm<tc::kEpiSplit>(X.mCuT[0], X.mCuT[1], X.mWt[0], X.mWt[1], Nu, Nphi, 2 * Nu, a, st));
+  // G4: dPhi[i][j] = phiscale[i] * Z[i][:] . Gphi[j][:]
+  a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi; a.row_scale = X.phiscale;
+  XK(gemm<tc::kEpiRowScaleF32>(X.mZ[0], X.mZ[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st));
+  return DG_OK;
+}
+
+int dg_handle::mixed_enqueue_step() {
+  MixedState &X = *mx;
+  const int c = cur, o = cur ^ 1;
+  int fm = kForceNone;
+  if (p.selfgrav) {
+    XK(prof_begin(DG_PROF_GRAVITY));
+    int rc = mixed_gravity();
+    if (rc) return rc;
+    XK(prof_end(DG_PROF_GRAVITY));
+    fm = kForcePhi;
+  }
+  dim3 grid((p.Nphi + kTJ32 - 1) / kTJ32, (p.Nu + kTI32 - 1) / kTI32);
+  XK(prof_begin(DG_PROF_HYDRO));
+  k_hydro32<<<grid, kHydro32Threads, 0, st>>>(X.sig[c], X.u[c], X.w[c], X.dPhi, nullptr, nullptr, fm, X.sig[o], X.u[o],
+                                              X.w[o], X.Sx, ctl, X.rows);
+  XK(cudaGetLastError());
+  XK(prof_end(DG_PROF_HYDRO));
+  cur = o;
+  return DG_OK;
+}
+
+int dg_handle::mixed_enqueue_step_forces(const double *gRh, const double *gph) {
+  MixedState &X = *mx;
+  const size_t n = (size_t)p.Nu * p.Nphi;
+  int fm = kForceNone;
+  if (gRh) {
+    // caller forces replace the self-gravity: subtract the basic-state gravity g0 from them
+    std::vector<double> a(gRh, gRh + n);
+    if (p.selfgrav)
+      for (int i = 0; i < p.Nu; ++i)
+        for (int j = 0; j < p.Nphi; ++j) a[(size_t)i * p.Nphi + j] -= X.g0[i];
+    XK(cudaMemcpyAsync(gA, a.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+    XK(cudaMemcpyAsync(gB, gph, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    XK(cudaStreamSynchronize(st));
+    fm = kForceArrays;
+  } else if (p.selfgrav) {
+    // no forces: the basic state loses its disk gravity too
+    std::vector<double> a(n);
+    for (int i = 0; i < p.Nu; ++i)
+      for (int j = 0; j < p.Nphi; ++j) a[(size_t)i * p.Nphi + j] = -X.g0[i];
+    std::vector<double> z(n, 0.0);
+    XK(cudaMemcpyAsync(gA, a.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+    XK(cudaMemcpyAsync(gB, z.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+    XK(cudaStreamSynchronize(st));
+    fm = kForceArrays;
+  }
+  const int c = cur, o = cur ^ 1;
+  dim3 grid((p.Nphi + kTJ32 - 1) / kTJ32, (p.Nu + kTI32 - 1) / kTI32);
+  k_hydro32<<<grid, kHydro32Threads, 0, st>>>(X.sig[c], X.u[c], X.w[c], nullptr, gA, gB, fm, X.sig[o], X.u[o], X.w[o],
+                                              X.Sx, ctl, X.rows);
+  XK(cudaGetLastError());
+  cur = o;
+  return DG_OK;
+}
+
+int dg_handle::mixed_cfl_launch(int nmodes, int record) {
+  MixedState &X = *mx;
+  const size_t n = (size_t)p.Nu * p.Nphi;
+  int blocks = grid_for(n);
+  if (blocks > 148 * 4) blocks = 148 * 4;
+  k_cfl32<<<blocks, 256, 0, st>>>(X.sig[cur], X.u[cur], X.w[cur], ctl, X.rows, nmodes, record);
+  XK(cudaGetLastError());
+  return DG_OK;
+}
+
+int dg_handle::mixed_modes_launch(int nmodes, double *out) {
+  MixedState &X = *mx;
+  const size_t n = (size_t)p.Nu * p.Nphi;
+  XK(cudaMemsetAsync(out, 0, 2 * nmodes * sizeof(double), st));
+  k_modes32<<<grid_for(n) < 592 ? grid_for(n) : 592, 256, 0, st>>>(X.sig[cur], X.rows, nmodes, out);
+  XK(cudaGetLastError());
+  return DG_OK;
+}
+
+int dg_handle::mixed_conserved_launch(double *out2) {
+  MixedState &X = *mx;
+  const size_t n = (size_t)p.Nu * p.Nphi;
+  XK(cudaMemsetAsync(out2, 0, 2 * sizeof(double), st));
+  k_conserved32<<<grid_for(n) < 592 ? grid_for(n) : 592, 256, 0, st>>>(X.sig[cur], X.w[cur], X.rows, out2);
+  XK(cudaGetLastError());
+  return DG_OK;
+}
+
+// dg_potential in mixed precision: the tensor-core convolution of a full field
+int dg_handle::mixed_potential(const double *dSig, double *dOut) {
+  MixedState &X = *mx;
+  const size_t n = (size_t)p.Nu * p.Nphi;
+  if (!have_state) {
+    // row tables are needed for R^{3/2}: build a trivial basic state
+    std::vector<double> S(n, 1.0), v(n, 0.0);
+    int rc = build_basic(this, S.data(), v.data());
+    if (rc) return rc;
+  }
+  k_full_to_sx<<<grid_for(n), 256, 0, st>>>(dSig, X.Sx, X.rows);
+  XK(cudaGetLastError());
+  int rc = mixed_gravity();
+  if (rc) return rc;
+  k_f32_to_f64<<<grid_for(n), 256, 0, st>>>(X.dPhi, dOut, n);
+  XK(cudaGetLastError());
+  // restore s of the current state for the next step
+  if (have_state) {
+    k_sig_to_sx<<<grid_for(n), 256, 0, st>>>(X.sig[cur], X.Sx, X.rows);
+    XK(cudaGetLastError());
+  }
+  return DG_OK;
+}

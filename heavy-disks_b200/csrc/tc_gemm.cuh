@@ -1,0 +1,284 @@
+// Split-BF16 tensor-core GEMM for sm_100a (tcgen05 + TMA + TMEM).
+//
+//   D[M x N] (FP32) = A[M x K] . B[N x K]^T,  A = A_hi + A_lo,  B = B_hi + B_lo (BF16 pairs)
+//   D ~= A_hi B_hi + A_hi B_lo + A_lo B_hi          (the A_lo B_lo term is below 2^-16 relative)
+//
+// Both operands are K-major (K contiguous) in global memory and are staged by TMA into
+// 128-byte-swizzled shared-memory tiles.  One thread issues the MMAs (three per 16-wide
+// K step, all accumulating into one FP32 TMEM accumulator); one thread drives TMA; the
+// four warps then drain TMEM through tcgen05.ld and run a fused epilogue.  Every
+// mbarrier wait is bounded: on timeout the kernel raises kStTimeout in the caller's
+// status word, drains what it has in flight, frees its TMEM and returns.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "dg_common.cuh"
+
+namespace dg {
+namespace tc {
+
+constexpr int BM = 128;      // rows of a CTA tile (TMEM lanes)
+constexpr int BN = 64;       // columns of a CTA tile (TMEM columns)
+constexpr int BK = 64;       // K per stage: 64 BF16 = one 128-byte swizzle row
+constexpr int STAGES = 4;
+constexpr int kThreads = 128;
+constexpr uint32_t kTileA = BM * BK * 2;
+constexpr uint32_t kTileB = BN * BK * 2;
+constexpr uint32_t kStageBytes = 2 * kTileA + 2 * kTileB;
+constexpr uint32_t kTmemCols = 64;  // power of two >= 32 and >= BN
+constexpr size_t kSmemBytes = (size_t)STAGES * kStageBytes + 1024;
+
+enum EpiMode : int {
+  kEpiSplit = 0,        // out_hi/out_lo[row][col] = split(D)
+  kEpiSplitScaled = 1,  // out = split(D * table[row][col])
+  kEpiRowScaleF32 = 2,  // out_f32[row][col] = D * row_scale[row]
+};
+
+struct GemmArgs {
+  int M, N, K;
+  __nv_bfloat16 *out_hi, *out_lo;
+  float *out_f32;
+  int ldo;
+  const float *table;  // kEpiSplitScaled, row stride ldo
+  const float *row_scale;
+  int *status;         // kSt* bits raised on a bounded-wait timeout
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Bounded parity wait: gives up after ~1 s of SM clock and raises kStTimeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *status) {
+  const uint32_t addr = smem_u32(bar);
+  long long start = 0;
+  for (uint32_t it = 0;; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (it == 64) start = clock64();
+    if (it > 64 && clock64() - start > (1ll << 31)) {
+      if (status) atomicOr(status, kStTimeout);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, uint64_t *bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          smem_u32(dst)),
+      "l"((uint64_t)tm), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t sdesc_sw128(const void *p) {
+  uint64_t a = smem_u32(p);
+  uint64_t d = 0;
+  d |= (a >> 4) & 0x3FFFull;            // start address
+  d |= 1ull << 16;                      // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;     // stride byte offset: 8 rows x 128 B
+  d |= 1ull << 46;                      // descriptor version (sm_100)
+  d |= 2ull << 61;                      // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor: kind::f16, A = B = BF16, D = F32, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_gemm_split(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
+                 const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, GemmArgs args) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], done_bar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int nk = args.K / BK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&done_bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tmem_alloc(&tmem_slot, kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_d = tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer ----
+    int issued = 0;
+    for (int kc = 0; kc < nk; ++kc) {
+      const int s = kc % STAGES;
+      if (kc >= STAGES && !mbar_wait(&empty_bar[s], ((kc / STAGES) - 1) & 1, args.status)) {
+        abort_flag = 1;
+        break;
+      }
+      if (abort_flag) break;
+      uint8_t *st = smem + s * kStageBytes;
+      mbar_arrive_expect_tx(&full_bar[s], kStageBytes);
+      tma_load_2d(st, &tmAh, &full_bar[s], kc * BK, m0);
+      tma_load_2d(st + kTileA, &tmAl, &full_bar[s], kc * BK, m0);
+      tma_load_2d(st + 2 * kTileA, &tmBh, &full_bar[s], kc * BK, n0);
+      tma_load_2d(st + 2 * kTileA + kTileB, &tmBl, &full_bar[s], kc * BK, n0);
+      ++issued;
+    }
+    // every issued copy must land before the CTA may exit
+    for (int kc = issued > STAGES ? issued - STAGES : 0; kc < issued; ++kc)
+      mbar_wait(&full_bar[kc % STAGES], (kc / STAGES) & 1, args.status);
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    const uint32_t idesc = idesc_bf16(BM, BN);
+    for (int kc = 0; kc < nk; ++kc) {
+      const int s = kc % STAGES;
+      if (!mbar_wait(&full_bar[s], (kc / STAGES) & 1, args.status)) {
+        abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      uint8_t *st = smem + s * kStageBytes;
+      const uint64_t dAh = sdesc_sw128(st), dAl = sdesc_sw128(st + kTileA);
+      const uint64_t dBh = sdesc_sw128(st + 2 * kTileA), dBl = sdesc_sw128(st + 2 * kTileA + kTileB);
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk) {
+        const uint64_t off = (uint64_t)((kk * 32) >> 4);
+        mma_bf16(tmem_d, dAh + off, dBh + off, idesc, (kc | kk) != 0);
+        mma_bf16(tmem_d, dAh + off, dBl + off, idesc, 1u);
+        mma_bf16(tmem_d, dAl + off, dBh + off, idesc, 1u);
+      }
+      mma_commit(&empty_bar[s]);
+    }
+    mma_commit(&done_bar);  // arrives once every MMA issued above has completed
+  }
+  __syncwarp();
+
+  // ---- epilogue: TMEM lanes 32w..32w+31 belong to warp w ----
+  const bool ok = mbar_wait(&done_bar, 0, args.status);
+  tc_fence_after();
+  if (ok && !abort_flag) {
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+      uint32_t r[32];
+      tmem_ld32(tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
+      const int col = n0 + c0;
+      if (MODE == kEpiRowScaleF32) {
+        const float sc = args.row_scale[row];
+        float4 *o = reinterpret_cast<float4 *>(args.out_f32 + (size_t)row * args.ldo + col);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          o[q] = make_float4(__uint_as_float(r[4 * q]) * sc, __uint_as_float(r[4 * q + 1]) * sc,
+                             __uint_as_float(r[4 * q + 2]) * sc, __uint_as_float(r[4 * q + 3]) * sc);
+      } else {
+        float v[32];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
+        if (MODE == kEpiSplitScaled) {
+          const float4 *tb = reinterpret_cast<const float4 *>(args.table + (size_t)row * args.ldo + col);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            float4 t = tb[q];
+            v[4 * q] *= t.x; v[4 * q + 1] *= t.y; v[4 * q + 2] *= t.z; v[4 * q + 3] *= t.w;
+          }
+        }
+        uint32_t ph[16], pl[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          __nv_bfloat16 h0, l0, h1, l1;
+          split_bf16(v[2 * q], h0, l0);
+          split_bf16(v[2 * q + 1], h1, l1);
+          ph[q] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+          pl[q] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+        }
+        uint4 *oh = reinterpret_cast<uint4 *>(args.out_hi + (size_t)row * args.ldo + col);
+        uint4 *ol = reinterpret_cast<uint4 *>(args.out_lo + (size_t)row * args.ldo + col);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          oh[q] = make_uint4(ph[4 * q], ph[4 * q + 1], ph[4 * q + 2], ph[4 * q + 3]);
+          ol[q] = make_uint4(pl[4 * q], pl[4 * q + 1], pl[4 * q + 2], pl[4 * q + 3]);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem_d, kTmemCols);
+}
+
+}  // namespace tc
+}  // namespace dg

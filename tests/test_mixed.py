@@ -1,0 +1,108 @@
+"""Mixed-precision path (FP32 perturbation about an FP64 basic state, split-BF16 tcgen05
+DFT gravity) against the FP64 oracle.
+
+Tolerances (stated per check): the split-BF16 products carry ~2^-16 relative error per
+term, so the gravity of a field agrees with the FP64 potential to <= 2e-4 relative; the
+perturbation fields after 100 steps agree to <= 2e-3 of the perturbation's own size;
+gamma and Omega_p from the same run agree to <= 0.5 %."""
+import numpy as np
+import pytest
+
+import diskgpu as D
+import oracle as O
+from diskgpu.analysis import fit_growth
+from helpers import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _field(Nu, Nphi, seed=0):
+    rng = np.random.default_rng(seed)
+    R = np.exp(np.log(0.25) + (np.arange(Nu) + 0.5) * np.log(4.0) / Nu)
+    phi = (np.arange(Nphi) + 0.5) * 2 * np.pi / Nphi
+    S0 = 0.372 * np.exp(-(R - 0.45) ** 2 / 0.05)
+    pert = 0.05 * np.cos(2 * phi)[None, :] + 0.02 * np.sin(3 * phi + 1)[None, :] * np.sin(7 * R)[:, None]
+    return S0[:, None] * (1 + pert) + 1e-3 * rng.random((Nu, Nphi))
+
+
+@pytest.mark.parametrize("Nu,Nphi", [(128, 128), (256, 256), (128, 384), (512, 256)])
+def test_tensor_core_potential_vs_fp64(Nu, Nphi):
+    """The 4-GEMM split-BF16 DFT convolution against the FP64 FFT potential (<= 2e-4 rel)."""
+    Sig = _field(Nu, Nphi)
+    ref = O.Kalnajs(Nu, Nphi, eps=0.01).potential(Sig)
+    with D.Disk(Nu, Nphi, eps=0.01, precision="mixed") as d:
+        got = d.potential(Sig)
+    assert rel_err(got, ref) < 2e-4
+    # the non-axisymmetric part alone (what the mixed step actually convolves)
+    pert = Sig - Sig.mean(axis=1, keepdims=True)
+    refp = O.Kalnajs(Nu, Nphi, eps=0.01).potential(pert)
+    with D.Disk(Nu, Nphi, eps=0.01, precision="mixed") as d:
+        gotp = d.potential(pert)
+    assert rel_err(gotp, refp) < 2e-4
+
+
+def test_state_roundtrip_mixed():
+    with D.Disk(128, 128, eps=0.01, precision="mixed") as d:
+        d.init_standard()
+        S, vR, vp = d.get_state()
+        ref = O.Disk(Nu=128, Nphi=128, eps=0.01)
+        Sr, vRr, vpr = ref.hyd.state()
+        # the perturbation (amp 1e-3 of Sigma0) survives FP32 storage to ~1e-7 of itself
+        pr = Sr - Sr.mean(axis=1, keepdims=True)
+        assert np.max(np.abs((S - Sr))) <= 1e-6 * np.max(np.abs(pr))
+        assert rel_err(vp, vpr) < 1e-12
+        m, L = d.conserved()
+        assert m == pytest.approx(ref.mD, rel=1e-12)
+
+
+@pytest.mark.parametrize("N,steps", [(256, 100), (128, 200)])
+def test_mixed_vs_fp64_after_steps(N, steps):
+    ref = O.Disk(Nu=N, Nphi=N, eps=0.005, amp=1e-3, nthreads=8)
+    S0 = ref.hyd.get("Sig").mean(axis=1, keepdims=True)
+    with D.Disk(N, N, eps=0.005, amp=1e-3, precision="mixed") as d:
+        d.init_standard()
+        for _ in range(steps):
+            dt_ref = ref.step()
+            dt = d.timestep(0.3)
+            assert abs(dt - dt_ref) <= 1e-5 * dt_ref
+            d.step(dt_ref)
+        S, vR, vp = d.get_state()
+    Sr, vRr, vpr = ref.hyd.state()
+    # errors measured against the size of the perturbation itself
+    assert np.max(np.abs(S - Sr)) <= 2e-3 * np.max(np.abs(Sr - S0))
+    assert np.max(np.abs(vR - vRr)) <= 2e-3 * np.max(np.abs(vRr))
+    vp0 = vpr.mean(axis=1, keepdims=True)
+    assert np.max(np.abs(vp - vpr)) <= 2e-3 * np.max(np.abs(vpr - vp0)) + 1e-9
+
+
+def test_growth_rate_and_pattern_speed_match_fp64():
+    """gamma, Omega_p of the m=2 mode from mixed and FP64 runs of the same disk (<= 0.5 %)."""
+    kw = dict(eps=0.01, amp=1e-3)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with D.Disk(128, 128, precision=prec, **kw) as d:
+            d.init_standard()
+            rec, t, n = d.advance(6.0)
+        out[prec] = fit_growth(rec[:, 0], rec[:, 2], rec[:, 3], tmin=2.0, tmax=6.0)
+    g64, w64, _ = out["fp64"]
+    gmx, wmx, _ = out["mixed"]
+    assert g64 > 0.2
+    assert abs(gmx - g64) <= 5e-3 * abs(g64)
+    assert abs(wmx - w64) <= 5e-3 * abs(w64)
+
+
+def test_mixed_requires_multiple_of_128():
+    with pytest.raises(D.DiskGPUError) as e:
+        D.Disk(96, 128, precision="mixed")
+    assert e.value.code == -4
+
+
+def test_mixed_nonfinite_reported():
+    with D.Disk(128, 128, precision="mixed") as d:
+        d.init_standard()
+        S, vR, vp = d.get_state()
+        vR[3, 3] = np.inf
+        d.set_state(S, vR, vp)
+        with pytest.raises(D.DiskGPUError) as e:
+            d.run_steps(3)
+        assert e.value.code == -3
