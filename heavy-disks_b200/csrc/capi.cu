@@ -121,9 +121,32 @@ int dg_handle::init(const dg_params &pp) {
   MK(cudaMallocHost((void **)&hctl, sizeof(Ctl)));
   memset(hctl, 0, sizeof(Ctl));
   MK(cudaMallocHost((void **)&hdt, sizeof(double)));
+  {
+    // per-row / per-face FP64 constants of the hydro kernel
+    std::vector<double> t((size_t)8 * (Nu + 1), 0.0);
+    auto col = [&](int k) { return t.data() + (size_t)k * (Nu + 1); };
+    for (int i = 0; i < Nu; ++i) {
+      int im = i - 1 > 0 ? i - 1 : 0, ip = i + 1 < Nu - 1 ? i + 1 : Nu - 1;
+      col(0)[i] = -p.gmstar / (R[i] * R[i]);
+      col(1)[i] = 1.0 / R[i];
+      col(2)[i] = 1.0 / (R[ip] - R[im]);
+      col(3)[i] = 1.0 / Vol[i];
+      col(4)[i] = 1.0 / (Rf[i + 1] - Rf[i]);
+      col(5)[i] = 1.0 / (R[i] * dphi);
+    }
+    for (int f = 1; f <= Nu; ++f) col(6)[f] = 1.0 / (Rf[f] - Rf[f - 1]);
+    for (int f = 0; f < Nu; ++f) col(7)[f] = 1.0 / (Rf[f + 1] - Rf[f]);
+    MK(dmalloc(&rowtab, t.size()));
+    MK(cudaMemcpy(rowtab, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+    auto dc = [&](int k) { return (const double *)(rowtab + (size_t)k * (Nu + 1)); };
+    geom.gstar = dc(0); geom.invR = dc(1); geom.invdRc = dc(2); geom.invVol = dc(3);
+    geom.invdR = dc(4); geom.invdl = dc(5); geom.invdRl = dc(6); geom.invdRr = dc(7);
+  }
   geom.R = dR; geom.Rf = dRf; geom.Vol = dVol;
   geom.Nu = Nu; geom.Nphi = Nphi; geom.dphi = dphi; geom.du = du;
   geom.Kpoly = p.Kpoly; geom.gamma = p.gamma_gas; geom.gmstar = p.gmstar;
+  geom.inv2dphi = 1.0 / (2.0 * dphi); geom.invdu = 1.0 / du; geom.inv2du = 1.0 / (2.0 * du);
+  geom.gamma2 = (p.gamma_gas == 2.0) ? 1 : 0;
   MK(prepare_fft_kernels());
   int rc = build_khat();
   if (rc) return rc;
@@ -152,7 +175,7 @@ void dg_handle::release() {
   if (st) cudaStreamSynchronize(st);
   mixed_release();
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
-  void *ptrs[] = {dR, dRf, dVol, dSqrtR, dR32, S[0], S[1], VR[0], VR[1], VP[0], VP[1], dPhi, gA, gB,
+  void *ptrs[] = {rowtab, dR, dRf, dVol, dSqrtR, dR32, S[0], S[1], VR[0], VR[1], VP[0], VP[1], dPhi, gA, gB,
                   W, Khat, rootsPhi, rootsM, scratch, ctl};
   for (void *q : ptrs)
     if (q) cudaFree(q);

@@ -24,6 +24,7 @@ struct dg_handle {
   int M = 0, Nc = 0;
   std::vector<double> R, Rf, Vol, sqrtR, R32;
   double *dR = nullptr, *dRf = nullptr, *dVol = nullptr, *dSqrtR = nullptr, *dR32 = nullptr;
+  double *rowtab = nullptr;  // per-row / per-face constants of the FP64 hydro kernel
   dg::Geom64 geom{};
 
   // plain-method state (ping-pong), forces scratch, gravity workspace

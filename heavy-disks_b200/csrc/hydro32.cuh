@@ -28,6 +28,7 @@ struct Rows32 {
   const double *S0d, *V0d, *Rd, *dAd;  // FP64 copies for the global sums
   // faces f in [0, Nu]
   const float *Af, *dRl, *dRr, *dV, *dS0;
+  const float *invdR, *invdl, *invdRl, *invdRr;  // reciprocals (rows, rows, faces, faces)
   int Nu, Nphi;
   float dphi, inv2dphi, invdu, inv2du, Kpoly, gamma, gmstar;
   int gamma2;  // gamma == 2: P = K Sigma^2 exactly
@@ -38,7 +39,10 @@ constexpr int kLI32 = kTI32 + 2 * kH32, kLJ32 = kTJ32 + 2 * kH32;
 constexpr int kSI32 = kTI32 + 4, kSJ32 = kTJ32 + 4;
 constexpr int kHydro32Threads = 256;
 
-__device__ __forceinline__ float vanleer32(float a, float b) { return (a * b > 0.f) ? 2.f * a * b / (a + b) : 0.f; }
+// hydro.hpp:16-18; a*b > 0 means |a + b| >= max(|a|, |b|) > 0, so the fast divide is safe
+__device__ __forceinline__ float vanleer32(float a, float b) {
+  return (a * b > 0.f) ? __fdividef(2.f * a * b, a + b) : 0.f;
+}
 
 // P(Sigma0 + s) - P(Sigma0) for P = K Sigma^gamma
 __device__ __forceinline__ float dpres32(const Rows32 &g, int i, float s) {
@@ -51,7 +55,7 @@ __device__ __forceinline__ float cfl_rate32(const Rows32 &g, int i, float sig, f
   s = (s < 1e-12f) ? 1e-12f : s;
   float cs2 = g.gamma2 ? g.gamma * g.Kpoly * s : g.gamma * g.Kpoly * powf(s, g.gamma - 1.f);
   float cs = sqrtf(cs2);
-  return (fabsf(u) + cs) / g.dR[i] + (fabsf(g.V0[i] + w) + cs) / g.dl[i];
+  return (fabsf(u) + cs) * g.invdR[i] + (fabsf(g.V0[i] + w) + cs) * g.invdl[i];
 }
 
 }  // namespace dg

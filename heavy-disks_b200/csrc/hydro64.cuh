@@ -21,8 +21,14 @@ namespace dg {
 
 struct Geom64 {
   const double *R, *Rf, *Vol;
+  // per-row constants: -GM*/R^2, 1/R, 1/(R[ip]-R[im]), 1/Vol, 1/(Rf[i+1]-Rf[i]), 1/(R dphi)
+  const double *gstar, *invR, *invdRc, *invVol, *invdR, *invdl;
+  // per-face constants: 1/(Rf[f]-Rf[f-1]), 1/(Rf[f+1]-Rf[f])
+  const double *invdRl, *invdRr;
   int Nu, Nphi;
   double dphi, du, Kpoly, gamma, gmstar;
+  double inv2dphi, invdu, inv2du;
+  int gamma2;  // gamma == 2: P = K s^2, cs^2 = 2 K s without pow
 };
 
 // Which self-gravity the kernel applies (hydro.hpp:86-88).
@@ -39,17 +45,16 @@ __device__ __forceinline__ double vanleer64(double a, double b) {  // hydro.hpp:
 __device__ __forceinline__ double dmax_ref(double a, double b) { return (a < b) ? b : a; }  // std::max
 
 __device__ __forceinline__ double pres64(const Geom64 &g, double s) {  // hydro.hpp:46
-  return g.Kpoly * pow(s, g.gamma);
+  return g.gamma2 ? g.Kpoly * (s * s) : g.Kpoly * pow(s, g.gamma);
 }
 __device__ __forceinline__ double cs2_64(const Geom64 &g, double s) {  // hydro.hpp:45
-  return g.gamma * g.Kpoly * pow(s, g.gamma - 1.0);
+  return g.gamma2 ? g.gamma * g.Kpoly * s : g.gamma * g.Kpoly * pow(s, g.gamma - 1.0);
 }
 // (|vR| + cs)/dR + (|vp| + cs)/(R dphi)  (hydro.hpp:54-57)
 __device__ __forceinline__ double cfl_rate64(const Geom64 &g, int i, double s, double vr, double vp) {
-  double dR = g.Rf[i + 1] - g.Rf[i];
   double cs = sqrt(cs2_64(g, dmax_ref(s, 1e-12)));
-  double sR = (fabs(vr) + cs) / dR;
-  double sp = (fabs(vp) + cs) / (g.R[i] * g.dphi);
+  double sR = (fabs(vr) + cs) * g.invdR[i];
+  double sp = (fabs(vp) + cs) * g.invdl[i];
   return sR + sp;
 }
 

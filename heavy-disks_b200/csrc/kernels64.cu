@@ -84,21 +84,20 @@ __global__ void __launch_bounds__(kHydroThreads) k_hydro64(
     if (i >= 0 && i < Nu) {
       int im = i - 1 > 0 ? i - 1 : 0, ip = i + 1 < Nu - 1 ? i + 1 : Nu - 1;
       int lim = li + (im - i), lip = li + (ip - i);
-      double Ri = g.R[i];
-      double dRc = g.R[ip] - g.R[im];
+      double Ri = g.R[i], iR = g.invR[i];
       double s = sS[li][lj];
-      double dPdR = (sP[lip][lj] - sP[lim][lj]) / dRc;
-      double dPdphi = (sP[li][lj + 1] - sP[li][lj - 1]) / (2.0 * g.dphi);
-      double gR = -g.gmstar / (Ri * Ri);
+      double dPdR = (sP[lip][lj] - sP[lim][lj]) * g.invdRc[i];
+      double dPdphi = (sP[li][lj + 1] - sP[li][lj - 1]) * g.inv2dphi;
+      double gR = g.gstar[i];
       double gp = 0.0;
       if (force_mode == kForcePhi) {  // kalnajs.hpp:71-78
-        double dPhidphi = (sPh[li][lj + 1] - sPh[li][lj - 1]) / (2.0 * g.dphi);
+        double dPhidphi = (sPh[li][lj + 1] - sPh[li][lj - 1]) * g.inv2dphi;
         double dPhidu;
-        if (i == 0) dPhidu = (sPh[li + 1][lj] - sPh[li][lj]) / g.du;
-        else if (i == Nu - 1) dPhidu = (sPh[li][lj] - sPh[li - 1][lj]) / g.du;
-        else dPhidu = (sPh[li + 1][lj] - sPh[li - 1][lj]) / (2.0 * g.du);
-        gR += -dPhidu / Ri;
-        gp += -dPhidphi / Ri;
+        if (i == 0) dPhidu = (sPh[li + 1][lj] - sPh[li][lj]) * g.invdu;
+        else if (i == Nu - 1) dPhidu = (sPh[li][lj] - sPh[li - 1][lj]) * g.invdu;
+        else dPhidu = (sPh[li + 1][lj] - sPh[li - 1][lj]) * g.inv2du;
+        gR += -dPhidu * iR;
+        gp += -dPhidphi * iR;
       } else if (force_mode == kForceArrays) {
         int j = ((j0 - 2 + sj) % Nphi + Nphi) % Nphi;
         size_t k = (size_t)i * Nphi + j;
@@ -106,8 +105,8 @@ __global__ void __launch_bounds__(kHydroThreads) k_hydro64(
         gp += gpin[k];
       }
       double vrc = sVR[li][lj], vpc = sVP[li][lj];
-      double aR = -dPdR / s + gR + vpc * vpc / Ri;
-      double ap = -(1.0 / (s * Ri)) * dPdphi + gp - vrc * vpc / Ri;
+      double aR = -dPdR / s + gR + vpc * vpc * iR;
+      double ap = -(1.0 / (s * Ri)) * dPdphi + gp - vrc * vpc * iR;
       nvr = vrc + dt * aR;
       nvp = vpc + dt * ap;
     }
@@ -127,7 +126,7 @@ __global__ void __launch_bounds__(kHydroThreads) k_hydro64(
     double F = 0.0, FR = 0.0, FP = 0.0;
     if (f >= 1 && f <= Nu - 1) {
       double Af = g.Rf[f] * g.dphi;
-      double dRl = g.Rf[f] - g.Rf[f - 1], dRr = g.Rf[f + 1] - g.Rf[f];
+      double idRl = g.invdRl[f], idRr = g.invdRr[f];
       double vf = 0.5 * (VRsrc(f - 1, sj) + VRsrc(f, sj));
       double sf, vRf, vpf;
       if (vf > 0) {
@@ -136,18 +135,18 @@ __global__ void __launch_bounds__(kHydroThreads) k_hydro64(
         double kS = sl ? vanleer64(Ssrc(u + 1, sj) - Ssrc(u, sj), Ssrc(u, sj) - Ssrc(u - 1, sj)) : 0.0;
         double kR = sl ? vanleer64(VRsrc(u + 1, sj) - VRsrc(u, sj), VRsrc(u, sj) - VRsrc(u - 1, sj)) : 0.0;
         double kP = sl ? vanleer64(VPsrc(u + 1, sj) - VPsrc(u, sj), VPsrc(u, sj) - VPsrc(u - 1, sj)) : 0.0;
-        sf = Ssrc(u, sj) + 0.5 * kS * (1.0 - vf * dt / dRl);
-        vRf = VRsrc(u, sj) + 0.5 * kR * (1.0 - vf * dt / dRl);
-        vpf = VPsrc(u, sj) + 0.5 * kP * (1.0 - vf * dt / dRl);
+        sf = Ssrc(u, sj) + 0.5 * kS * (1.0 - vf * dt * idRl);
+        vRf = VRsrc(u, sj) + 0.5 * kR * (1.0 - vf * dt * idRl);
+        vpf = VPsrc(u, sj) + 0.5 * kP * (1.0 - vf * dt * idRl);
       } else {
         int u = f;
         bool sl = (u > 0 && u < Nu - 1);
         double kS = sl ? vanleer64(Ssrc(u + 1, sj) - Ssrc(u, sj), Ssrc(u, sj) - Ssrc(u - 1, sj)) : 0.0;
         double kR = sl ? vanleer64(VRsrc(u + 1, sj) - VRsrc(u, sj), VRsrc(u, sj) - VRsrc(u - 1, sj)) : 0.0;
         double kP = sl ? vanleer64(VPsrc(u + 1, sj) - VPsrc(u, sj), VPsrc(u, sj) - VPsrc(u - 1, sj)) : 0.0;
-        sf = Ssrc(u, sj) - 0.5 * kS * (1.0 + vf * dt / dRr);
-        vRf = VRsrc(u, sj) - 0.5 * kR * (1.0 + vf * dt / dRr);
-        vpf = VPsrc(u, sj) - 0.5 * kP * (1.0 + vf * dt / dRr);
+        sf = Ssrc(u, sj) - 0.5 * kS * (1.0 + vf * dt * idRr);
+        vRf = VRsrc(u, sj) - 0.5 * kR * (1.0 + vf * dt * idRr);
+        vpf = VPsrc(u, sj) - 0.5 * kP * (1.0 + vf * dt * idRr);
       }
       double fm = vf * sf * Af;
       F = fm; FR = fm * vRf; FP = fm * vpf;
@@ -164,10 +163,10 @@ __global__ void __launch_bounds__(kHydroThreads) k_hydro64(
     if (i < Nu) {
       double s = Ssrc(i, sj), vr1 = VRsrc(i, sj), vp1 = VPsrc(i, sj);
       double mR = s * vr1, mp = s * vp1;
-      double V = g.Vol[i];
-      ns = s + dt * (fF[ri][sj] - fF[ri + 1][sj]) / V;
-      double nmR = mR + dt * (fFR[ri][sj] - fFR[ri + 1][sj]) / V;
-      double nmP = mp + dt * (fFP[ri][sj] - fFP[ri + 1][sj]) / V;
+      double iV = g.invVol[i];
+      ns = s + dt * (fF[ri][sj] - fF[ri + 1][sj]) * iV;
+      double nmR = mR + dt * (fFR[ri][sj] - fFR[ri + 1][sj]) * iV;
+      double nmP = mp + dt * (fFP[ri][sj] - fFP[ri + 1][sj]) * iV;
       double d = dmax_ref(ns, 1e-10);
       a = nmR / d;
       b = nmP / d;
@@ -183,7 +182,7 @@ __global__ void __launch_bounds__(kHydroThreads) k_hydro64(
     int i = i0 + ri;
     double F = 0.0, FR = 0.0, FP = 0.0;
     if (i < Nu) {
-      double dl = g.R[i] * g.dphi, Aface = g.Rf[i + 1] - g.Rf[i];
+      double idl = g.invdl[i], Aface = g.Rf[i + 1] - g.Rf[i];
       int cm = pj + 1, cc = pj + 2;  // cells j-1, j
       double vf = 0.5 * (s2VP[ri][cm] + s2VP[ri][cc]);
       double sf, vRf, vpf;
@@ -192,13 +191,13 @@ __global__ void __launch_bounds__(kHydroThreads) k_hydro64(
       double kR = vanleer64(s2VR[ri][u + 1] - s2VR[ri][u], s2VR[ri][u] - s2VR[ri][u - 1]);
       double kP = vanleer64(s2VP[ri][u + 1] - s2VP[ri][u], s2VP[ri][u] - s2VP[ri][u - 1]);
       if (vf > 0) {
-        sf = s2S[ri][u] + 0.5 * kS * (1.0 - vf * dt / dl);
-        vRf = s2VR[ri][u] + 0.5 * kR * (1.0 - vf * dt / dl);
-        vpf = s2VP[ri][u] + 0.5 * kP * (1.0 - vf * dt / dl);
+        sf = s2S[ri][u] + 0.5 * kS * (1.0 - vf * dt * idl);
+        vRf = s2VR[ri][u] + 0.5 * kR * (1.0 - vf * dt * idl);
+        vpf = s2VP[ri][u] + 0.5 * kP * (1.0 - vf * dt * idl);
       } else {
-        sf = s2S[ri][u] - 0.5 * kS * (1.0 + vf * dt / dl);
-        vRf = s2VR[ri][u] - 0.5 * kR * (1.0 + vf * dt / dl);
-        vpf = s2VP[ri][u] - 0.5 * kP * (1.0 + vf * dt / dl);
+        sf = s2S[ri][u] - 0.5 * kS * (1.0 + vf * dt * idl);
+        vRf = s2VR[ri][u] - 0.5 * kR * (1.0 + vf * dt * idl);
+        vpf = s2VP[ri][u] - 0.5 * kP * (1.0 + vf * dt * idl);
       }
       double fm = vf * sf * Aface;
       F = fm; FR = fm * vRf; FP = fm * vpf;
@@ -216,10 +215,10 @@ __global__ void __launch_bounds__(kHydroThreads) k_hydro64(
       int cc = pj + 2;
       double s = s2S[ri][cc], vr = s2VR[ri][cc], vpp = s2VP[ri][cc];
       double mR = s * vr, mp = s * vpp;
-      double V = g.Vol[i];
-      double ns = s + dt * (pF[ri][pj] - pF[ri][pj + 1]) / V;
-      double nmR = mR + dt * (pF[kTI + ri][pj] - pF[kTI + ri][pj + 1]) / V;
-      double nmP = mp + dt * (pF[2 * kTI + ri][pj] - pF[2 * kTI + ri][pj + 1]) / V;
+      double iV = g.invVol[i];
+      double ns = s + dt * (pF[ri][pj] - pF[ri][pj + 1]) * iV;
+      double nmR = mR + dt * (pF[kTI + ri][pj] - pF[kTI + ri][pj + 1]) * iV;
+      double nmP = mp + dt * (pF[2 * kTI + ri][pj] - pF[2 * kTI + ri][pj + 1]) * iV;
       double d = dmax_ref(ns, 1e-10);
       double vro = nmR / d, vpo_ = nmP / d;
       double so = dmax_ref(ns, 1e-10);

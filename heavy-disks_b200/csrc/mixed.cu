@@ -183,11 +183,11 @@ __global__ void k_from_pert(const float *sig, const float *u, const float *w, do
 }
 
 // s = R^{3/2} Sigma of a full FP64 field (dg_potential in mixed precision)
-__global__ void k_full_to_sx(const double *S, SplitBuf Sx, Rows32 g) {
-  const size_t n = (size_t)g.Nu * g.Nphi;
+__global__ void k_full_to_sx(const double *S, SplitBuf Sx, const double *R32d, int Nu, int Nphi) {
+  const size_t n = (size_t)Nu * Nphi;
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
-    int i = (int)(k / g.Nphi);
-    float x = (float)((double)g.R32[i] * S[k]);
+    int i = (int)(k / Nphi);
+    float x = (float)(R32d[i] * S[k]);
     __nv_bfloat16 h = __float2bfloat16_rn(x);
     Sx.hi[k] = h;
     Sx.lo[k] = __float2bfloat16_rn(x - __bfloat162float(h));
@@ -302,8 +302,9 @@ __global__ void __launch_bounds__(kHydro32Threads) k_hydro32(const float *__rest
       }
       const float uc = sU[li][lj], wc = sW[li][lj];
       const float V = g.V0[i];
-      const float aR = g.a0[i] + (g.dP0dR[i] * sg * g.invS0[i] - ddP) / s + dgR + (2.f * V + wc) * wc * g.invR[i];
-      const float ap = -dPdphi / (s * g.R[i]) + dgp - uc * (V + wc) * g.invR[i];
+      const float aR = g.a0[i] + __fdividef(g.dP0dR[i] * sg * g.invS0[i] - ddP, s) + dgR +
+                       (2.f * V + wc) * wc * g.invR[i];
+      const float ap = __fdividef(-dPdphi, s * g.R[i]) + dgp - uc * (V + wc) * g.invR[i];
       nu = uc + dt * aR;
       nw = wc + dt * ap;
     }
@@ -324,8 +325,8 @@ __global__ void __launch_bounds__(kHydro32Threads) k_hydro32(const float *__rest
       const float vf = 0.5f * (U1(f - 1, sj) + U1(f, sj));
       int cc;
       float hf;
-      if (vf > 0.f) { cc = f - 1; hf = 0.5f * (1.f - vf * dt / g.dRl[f]); }
-      else { cc = f; hf = -0.5f * (1.f + vf * dt / g.dRr[f]); }
+      if (vf > 0.f) { cc = f - 1; hf = 0.5f * (1.f - vf * dt * g.invdRl[f]); }
+      else { cc = f; hf = -0.5f * (1.f + vf * dt * g.invdRr[f]); }
       float kS = 0.f, kU = 0.f, kV = 0.f;
       if (cc > 0 && cc < Nu - 1) {
         kS = vanleer32(g.dS0[cc + 1] + (SG(cc + 1, sj) - SG(cc, sj)), g.dS0[cc] + (SG(cc, sj) - SG(cc - 1, sj)));
@@ -356,8 +357,8 @@ __global__ void __launch_bounds__(kHydro32Threads) k_hydro32(const float *__rest
       ns = sg + dt * (fF[ri][sj] - fF[ri + 1][sj]) * iv;
       float s2 = g.S0[i] + ns;
       float d = (s2 < 1e-10f) ? 1e-10f : s2;
-      a = (s * u1 + dt * (fFR[ri][sj] - fFR[ri + 1][sj]) * iv) / d;
-      b = (s * w1 + dt * (fGB[ri][sj] - fGA[ri + 1][sj]) * iv) / d;
+      a = __fdividef(s * u1 + dt * (fFR[ri][sj] - fFR[ri + 1][sj]) * iv, d);
+      b = __fdividef(s * w1 + dt * (fGB[ri][sj] - fGA[ri + 1][sj]) * iv, d);
     }
     s2S[ri][sj] = ns; s2U[ri][sj] = a; s2W[ri][sj] = b;
   }
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(kHydro32Threads) k_hydro32(const float *__rest
       const float dv = 0.5f * (s2W[ri][cm] + s2W[ri][cc]);
       const float vf = V + dv;
       const int up = (vf > 0.f) ? cm : cc;
-      const float hf = (vf > 0.f) ? 0.5f * (1.f - vf * dt / g.dl[i]) : -0.5f * (1.f + vf * dt / g.dl[i]);
+      const float hf = (vf > 0.f) ? 0.5f * (1.f - vf * dt * g.invdl[i]) : -0.5f * (1.f + vf * dt * g.invdl[i]);
       const float kS = vanleer32(s2S[ri][up + 1] - s2S[ri][up], s2S[ri][up] - s2S[ri][up - 1]);
       const float kU = vanleer32(s2U[ri][up + 1] - s2U[ri][up], s2U[ri][up] - s2U[ri][up - 1]);
       const float kW = vanleer32(s2W[ri][up + 1] - s2W[ri][up], s2W[ri][up] - s2W[ri][up - 1]);
@@ -405,8 +406,8 @@ __global__ void __launch_bounds__(kHydro32Threads) k_hydro32(const float *__rest
       float sg3 = sg2 + dt * (pF[ri][pj] - pF[ri][pj + 1]) * iv;
       const float s3 = S0 + sg3;
       const float d = (s3 < 1e-10f) ? 1e-10f : s3;
-      const float u3 = (s2 * u2 + dt * (pF[kTI32 + ri][pj] - pF[kTI32 + ri][pj + 1]) * iv) / d;
-      const float w3 = (s2 * w2 + dt * (pF[2 * kTI32 + ri][pj] - pF[2 * kTI32 + ri][pj + 1]) * iv) / d;
+      const float u3 = __fdividef(s2 * u2 + dt * (pF[kTI32 + ri][pj] - pF[kTI32 + ri][pj + 1]) * iv, d);
+      const float w3 = __fdividef(s2 * w2 + dt * (pF[2 * kTI32 + ri][pj] - pF[2 * kTI32 + ri][pj + 1]) * iv, d);
       if (s3 < 1e-10f) sg3 = 1e-10f - S0;  // floor (hydro.hpp:69)
       const size_t k = (size_t)i * Nphi + j;
       so[k] = sg3; uo[k] = u3; wo[k] = w3;
@@ -578,7 +579,7 @@ int dg_handle::mixed_init() {
   XK(dalloc(&X.KW, (size_t)Nphi * 2 * Nu));
   XK(dalloc(&X.dPhi, n));
   XK(dalloc(&X.phiscale, Nu));
-  XK(dalloc(&X.rowbuf, (size_t)20 * (Nu + 1)));
+  XK(dalloc(&X.rowbuf, (size_t)24 * (Nu + 1)));
   XK(dalloc(&X.rowbufd, (size_t)4 * Nu));
   // DFT tables
   k_tab_phi<<<grid_for((size_t)Nphi * Nphi), 256, 0, st>>>(X.Fphi, X.Gphi, Nphi);
@@ -681,7 +682,7 @@ static int build_basic(dg_handle *h, const double *Sig, const double *vp) {
     a0[i] = -dP0dR[i] / X.S0[i] + gR + X.V0[i] * X.V0[i] / R[i];
   }
   const int L = Nu + 1;
-  std::vector<float> rb((size_t)20 * L, 0.f);
+  std::vector<float> rb((size_t)24 * L, 0.f);
   auto col = [&](int k) { return rb.data() + (size_t)k * L; };
   for (int i = 0; i < Nu; ++i) {
     int im = i - 1 > 0 ? i - 1 : 0, ip = i + 1 < Nu - 1 ? i + 1 : Nu - 1;
@@ -699,6 +700,8 @@ static int build_basic(dg_handle *h, const double *Sig, const double *vp) {
     col(11)[i] = (float)(1.0 / Vol[i]);
     col(12)[i] = (float)h->R32[i];
     col(13)[i] = (float)P0[i];
+    col(19)[i] = (float)(1.0 / (Rf[i + 1] - Rf[i]));
+    col(20)[i] = (float)(1.0 / (R[i] * h->dphi));
   }
   for (int f = 0; f <= Nu; ++f) {
     col(14)[f] = (float)(Rf[f] * h->dphi);
@@ -706,6 +709,8 @@ static int build_basic(dg_handle *h, const double *Sig, const double *vp) {
     col(16)[f] = (f <= Nu - 1) ? (float)(Rf[f + 1] - Rf[f]) : 0.f;
     col(17)[f] = (f >= 1 && f <= Nu - 1) ? (float)(X.V0[f] - X.V0[f - 1]) : 0.f;
     col(18)[f] = (f >= 1 && f <= Nu - 1) ? (float)(X.S0[f] - X.S0[f - 1]) : 0.f;
+    col(21)[f] = (f >= 1) ? (float)(1.0 / (Rf[f] - Rf[f - 1])) : 0.f;
+    col(22)[f] = (f <= Nu - 1) ? (float)(1.0 / (Rf[f + 1] - Rf[f])) : 0.f;
   }
   std::vector<double> rd((size_t)4 * Nu);
   for (int i = 0; i < Nu; ++i) {
@@ -723,6 +728,7 @@ static int build_basic(dg_handle *h, const double *Sig, const double *vp) {
   g.R = dc(0); g.invR = dc(1); g.invdRc = dc(2); g.dP0dR = dc(3); g.S0 = dc(4); g.invS0 = dc(5); g.V0 = dc(6);
   g.a0 = dc(7); g.dR = dc(8); g.dl = dc(9); g.Aphi = dc(10); g.invVol = dc(11); g.R32 = dc(12); g.P0 = dc(13);
   g.Af = dc(14); g.dRl = dc(15); g.dRr = dc(16); g.dV = dc(17); g.dS0 = dc(18);
+  g.invdR = dc(19); g.invdl = dc(20); g.invdRl = dc(21); g.invdRr = dc(22);
   g.S0d = X.rowbufd; g.V0d = X.rowbufd + Nu; g.Rd = X.rowbufd + 2 * Nu; g.dAd = X.rowbufd + 3 * Nu;
   g.Nu = Nu; g.Nphi = Nphi;
   g.dphi = (float)h->dphi; g.inv2dphi = (float)(1.0 / (2.0 * h->dphi));
@@ -878,13 +884,7 @@ int dg_handle::mixed_conserved_launch(double *out2) {
 int dg_handle::mixed_potential(const double *dSig, double *dOut) {
   MixedState &X = *mx;
   const size_t n = (size_t)p.Nu * p.Nphi;
-  if (!have_state) {
-    // row tables are needed for R^{3/2}: build a trivial basic state
-    std::vector<double> S(n, 1.0), v(n, 0.0);
-    int rc = build_basic(this, S.data(), v.data());
-    if (rc) return rc;
-  }
-  k_full_to_sx<<<grid_for(n), 256, 0, st>>>(dSig, X.Sx, X.rows);
+  k_full_to_sx<<<grid_for(n), 256, 0, st>>>(dSig, X.Sx, dR32, p.Nu, p.Nphi);
   XK(cudaGetLastError());
   int rc = mixed_gravity();
   if (rc) return rc;
