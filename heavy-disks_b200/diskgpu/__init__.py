@@ -58,6 +58,7 @@ EXPORTS = (
     "dg_init_standard", "dg_set_state", "dg_get_state", "dg_timestep", "dg_step", "dg_step_forces",
     "dg_potential", "dg_forces", "dg_disk_mass", "dg_modes", "dg_conserved", "dg_advance", "dg_time",
     "dg_set_stream", "dg_run_steps", "dg_step_host", "dg_profile_enable", "dg_profile_read",
+    "dg_timestep_static",
 )
 
 PROF_HYDRO, PROF_GRAVITY, PROF_CFL, PROF_N = 0, 1, 2, 3
@@ -104,6 +105,8 @@ def lib():
     L.dg_step_host.argtypes = [H, C.c_double, D, D, D, D]
     L.dg_profile_enable.argtypes = [H, C.c_int]
     L.dg_profile_read.argtypes = [H, D, C.POINTER(C.c_longlong)]
+    L.dg_timestep_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double,
+                                     C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     _lib = L
     return L
 

@@ -152,6 +152,19 @@ int dg_profile_enable(dg_handle *h, int on);
 /* Accumulated milliseconds and launch counts per phase since the last read (resets). */
 int dg_profile_read(dg_handle *h, double *ms, long long *count);
 
+/* Allocation-free CFL time step.  No counterpart in the reference: it is the same
+ * dt = cfl / max_ij (sR + sphi) as dg_timestep, for callers that may not allocate device
+ * memory when they need it (while recording a CUDA graph, or when a pool or framework owns
+ * all device memory).  Sig, vR, vp (Nu x Nphi, FP64, row-major) and dt (one double) are
+ * DEVICE pointers owned by the caller; the grid is rebuilt from Nu, Nphi, Rin, Rout.  The
+ * call allocates nothing: its scratch is a static per-device array of 8192 row maxima, so
+ * Nu > 8192 returns DG_ERR_UNSUPPORTED.  The first call on a device looks up that array's
+ * address (make it before any stream capture).  Work is queued on `stream` (a
+ * cudaStream_t as void*, NULL = default stream); the call does not synchronise.  All calls
+ * share the scratch: calls that overlap on the GPU race. */
+int dg_timestep_static(const double *Sig, const double *vR, const double *vp, int Nu, int Nphi, double Rin,
+                       double Rout, double Kpoly, double gamma_gas, double cfl, double *dt, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

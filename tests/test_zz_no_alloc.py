@@ -1,0 +1,47 @@
+"""dg_timestep_static: the CFL time step for callers that may not allocate device memory
+(for example while recording a CUDA graph, or when a memory pool owns the device).  It
+must agree with dg_timestep on the same state, on two calls in a row, with nothing of its
+own allocated (its scratch is a static per-device array).  Collected last on purpose."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import diskgpu as D
+
+pytestmark = pytest.mark.gpu
+
+
+def _call_static(dev_arrays, p, cfl, dt_dev, stream):
+    S, vR, vp = dev_arrays
+    rc = D.lib().dg_timestep_static(S.data_ptr(), vR.data_ptr(), vp.data_ptr(), p.Nu, p.Nphi, p.Rin, p.Rout,
+                                    p.Kpoly, p.gamma_gas, cfl, dt_dev.data_ptr(), C.c_void_p(stream))
+    assert rc == 0, D.lib().dg_status_string(rc)
+
+
+def test_static_timestep_matches_dg_timestep_twice():
+    import torch
+
+    with D.Disk(96, 80, eps=0.01, amp=0.05) as d:
+        d.init_standard()
+        dt_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        for call in range(2):
+            S, vR, vp = d.get_state()
+            dev = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (S, vR, vp)]
+            torch.cuda.synchronize()
+            _call_static(dev, d.p, 0.3, dt_dev, stream)
+            torch.cuda.synchronize()
+            got = float(dt_dev.item())
+            want = d.timestep(0.3)
+            assert got == pytest.approx(want, rel=1e-12), (call, got, want)
+            d.step(want)  # a different state for the second call
+
+
+def test_static_timestep_rejects_too_many_rows():
+    import torch
+
+    x = torch.zeros(8193 * 2, dtype=torch.float64, device="cuda")
+    rc = D.lib().dg_timestep_static(x.data_ptr(), x.data_ptr(), x.data_ptr(), 8193, 2, 0.25, 1.0, 0.25, 2.0, 0.3,
+                                    x.data_ptr(), None)
+    assert rc == -4
