@@ -34,11 +34,6 @@ struct Rows32 {
   int gamma2;  // gamma == 2: P = K Sigma^2 exactly
 };
 
-constexpr int kTI32 = 16, kTJ32 = 32, kH32 = 3;
-constexpr int kLI32 = kTI32 + 2 * kH32, kLJ32 = kTJ32 + 2 * kH32;
-constexpr int kSI32 = kTI32 + 4, kSJ32 = kTJ32 + 4;
-constexpr int kHydro32Threads = 256;
-
 // hydro.hpp:16-18; a*b > 0 means |a + b| >= max(|a|, |b|) > 0, so the fast divide is safe
 __device__ __forceinline__ float vanleer32(float a, float b) {
   return (a * b > 0.f) ? __fdividef(2.f * a * b, a + b) : 0.f;

@@ -22,6 +22,7 @@
 #include "hydro32.cuh"
 #include "tc_gemm.cuh"
 #include "step_ctl.cuh"
+#include "hydro32w.cuh"
 
 using namespace dg;
 
@@ -209,229 +210,6 @@ __global__ void k_sig_to_sx(const float *sig, SplitBuf Sx, Rows32 g) {
 __global__ void k_f32_to_f64(const float *a, double *b, size_t n) {
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
     b[k] = (double)a[k];
-}
-
-// ---------------------------------------------------------------------------------
-// fused hydro step on the perturbation
-
-__global__ void __launch_bounds__(kHydro32Threads) k_hydro32(const float *__restrict__ sig, const float *__restrict__ uu,
-                                                              const float *__restrict__ ww, const float *__restrict__ Phi,
-                                                              const double *__restrict__ gRin,
-                                                              const double *__restrict__ gpin, int force_mode,
-                                                              float *__restrict__ so, float *__restrict__ uo,
-                                                              float *__restrict__ wo, SplitBuf Sx, Ctl *ctl, Rows32 g) {
-  __shared__ float sS[kLI32][kLJ32], sU[kLI32][kLJ32], sW[kLI32][kLJ32], sP[kLI32][kLJ32], sPh[kLI32][kLJ32];
-  __shared__ float sU1[kSI32][kSJ32], sW1[kSI32][kSJ32];
-  __shared__ float fF[kTI32 + 1][kSJ32], fFR[kTI32 + 1][kSJ32], fGA[kTI32 + 1][kSJ32], fGB[kTI32 + 1][kSJ32];
-  __shared__ float pF[3 * kTI32][kTJ32 + 1];
-  __shared__ double red[kHydro32Threads / 32];
-  float(*s2S)[kLJ32] = sP;  // transportR outputs reuse dead tiles
-  float(*s2U)[kLJ32] = sU;
-  float(*s2W)[kLJ32] = sW;
-
-  const int Nu = g.Nu, Nphi = g.Nphi;
-  const int i0 = blockIdx.y * kTI32, j0 = blockIdx.x * kTJ32;
-  const int tid = threadIdx.x;
-  const StepInfo si = read_step_info(ctl, true);
-  const int nmodes = si.nmodes;
-  const float dt = (float)si.dt;
-  double msum[2 * kMaxModes];
-#pragma unroll
-  for (int q = 0; q < 2 * kMaxModes; ++q) msum[q] = 0.0;
-  double lmax = 0.0;
-  bool bad = false;
-
-  if (!si.active) {
-    for (int c = tid; c < kTI32 * kTJ32; c += kHydro32Threads) {
-      int i = i0 + c / kTJ32, j = j0 + c % kTJ32;
-      if (i < Nu && j < Nphi) {
-        size_t k = (size_t)i * Nphi + j;
-        so[k] = sig[k]; uo[k] = uu[k]; wo[k] = ww[k];
-        lmax = fmax(lmax, (double)cfl_rate32(g, i, sig[k], uu[k], ww[k]));
-      }
-    }
-    finish_launch<kHydro32Threads>(ctl, si, lmax, msum, red);
-    return;
-  }
-
-  // ---- load halo region ----
-  for (int c = tid; c < kLI32 * kLJ32; c += kHydro32Threads) {
-    int li = c / kLJ32, lj = c % kLJ32;
-    int i = i0 - kH32 + li;
-    int j = j0 - kH32 + lj;
-    j = ((j % Nphi) + Nphi) % Nphi;
-    float s = 0.f, a = 0.f, b = 0.f, ph = 0.f, dp = 0.f;
-    if (i >= 0 && i < Nu) {
-      size_t k = (size_t)i * Nphi + j;
-      s = sig[k]; a = uu[k]; b = ww[k];
-      if (force_mode == kForcePhi) ph = Phi[k];
-      dp = dpres32(g, i, s);
-    }
-    sS[li][lj] = s; sU[li][lj] = a; sW[li][lj] = b; sPh[li][lj] = ph; sP[li][lj] = dp;
-  }
-  __syncthreads();
-
-  // ---- source on rows i0-2 .. i0+TI+1 ----
-  for (int c = tid; c < kSI32 * kSJ32; c += kHydro32Threads) {
-    int si_ = c / kSJ32, sj = c % kSJ32;
-    int i = i0 - 2 + si_;
-    int li = si_ + 1, lj = sj + 1;
-    float nu = 0.f, nw = 0.f;
-    if (i >= 0 && i < Nu) {
-      int im = i - 1 > 0 ? i - 1 : 0, ip = i + 1 < Nu - 1 ? i + 1 : Nu - 1;
-      int lim = li + (im - i), lip = li + (ip - i);
-      const float sg = sS[li][lj];
-      const float s = g.S0[i] + sg;
-      const float ddP = (sP[lip][lj] - sP[lim][lj]) * g.invdRc[i];
-      const float dPdphi = (sP[li][lj + 1] - sP[li][lj - 1]) * g.inv2dphi;
-      float dgR = 0.f, dgp = 0.f;
-      if (force_mode == kForcePhi) {
-        float dPhidu;
-        if (i == 0) dPhidu = (sPh[li + 1][lj] - sPh[li][lj]) * g.invdu;
-        else if (i == Nu - 1) dPhidu = (sPh[li][lj] - sPh[li - 1][lj]) * g.invdu;
-        else dPhidu = (sPh[li + 1][lj] - sPh[li - 1][lj]) * g.inv2du;
-        dgR = -dPhidu * g.invR[i];
-        dgp = -(sPh[li][lj + 1] - sPh[li][lj - 1]) * g.inv2dphi * g.invR[i];
-      } else if (force_mode == kForceArrays) {
-        int j = ((j0 - 2 + sj) % Nphi + Nphi) % Nphi;
-        size_t k = (size_t)i * Nphi + j;
-        // caller forces are full fields: their axisymmetric part is in a0 only when they
-        // equal the basic-state gravity, so apply them in full and drop g0 from a0
-        dgR = (float)gRin[k];
-        dgp = (float)gpin[k];
-      }
-      const float uc = sU[li][lj], wc = sW[li][lj];
-      const float V = g.V0[i];
-      const float aR = g.a0[i] + __fdividef(g.dP0dR[i] * sg * g.invS0[i] - ddP, s) + dgR +
-                       (2.f * V + wc) * wc * g.invR[i];
-      const float ap = __fdividef(-dPdphi, s * g.R[i]) + dgp - uc * (V + wc) * g.invR[i];
-      nu = uc + dt * aR;
-      nw = wc + dt * ap;
-    }
-    sU1[si_][sj] = nu;
-    sW1[si_][sj] = nw;
-  }
-  __syncthreads();
-
-  // ---- transportR fluxes at faces f = i0 .. i0+TI ----
-  auto SG = [&](int i, int sj) { return sS[i - (i0 - 2) + 1][sj + 1]; };
-  auto U1 = [&](int i, int sj) { return sU1[i - (i0 - 2)][sj]; };
-  auto W1 = [&](int i, int sj) { return sW1[i - (i0 - 2)][sj]; };
-  for (int c = tid; c < (kTI32 + 1) * kSJ32; c += kHydro32Threads) {
-    int fi = c / kSJ32, sj = c % kSJ32;
-    int f = i0 + fi;
-    float F = 0.f, FR = 0.f, GA = 0.f, GB = 0.f;
-    if (f >= 1 && f <= Nu - 1) {
-      const float vf = 0.5f * (U1(f - 1, sj) + U1(f, sj));
-      int cc;
-      float hf;
-      if (vf > 0.f) { cc = f - 1; hf = 0.5f * (1.f - vf * dt * g.invdRl[f]); }
-      else { cc = f; hf = -0.5f * (1.f + vf * dt * g.invdRr[f]); }
-      float kS = 0.f, kU = 0.f, kV = 0.f;
-      if (cc > 0 && cc < Nu - 1) {
-        kS = vanleer32(g.dS0[cc + 1] + (SG(cc + 1, sj) - SG(cc, sj)), g.dS0[cc] + (SG(cc, sj) - SG(cc - 1, sj)));
-        kU = vanleer32(U1(cc + 1, sj) - U1(cc, sj), U1(cc, sj) - U1(cc - 1, sj));
-        kV = vanleer32(g.dV[cc + 1] + (W1(cc + 1, sj) - W1(cc, sj)), g.dV[cc] + (W1(cc, sj) - W1(cc - 1, sj)));
-      }
-      const float Sf = g.S0[cc] + SG(cc, sj) + hf * kS;
-      const float uf = U1(cc, sj) + hf * kU;
-      const float Df = (cc == f ? g.dV[f] : 0.f) + W1(cc, sj) + hf * kV;  // vphi_f - V0(f-1)
-      F = vf * Sf * g.Af[f];
-      FR = F * uf;
-      GA = F * Df;
-      GB = F * (Df - g.dV[f]);
-    }
-    fF[fi][sj] = F; fFR[fi][sj] = FR; fGA[fi][sj] = GA; fGB[fi][sj] = GB;
-  }
-  __syncthreads();
-
-  // ---- transportR gather on rows i0 .. i0+TI-1 ----
-  for (int c = tid; c < kTI32 * kSJ32; c += kHydro32Threads) {
-    int ri = c / kSJ32, sj = c % kSJ32;
-    int i = i0 + ri;
-    float ns = 0.f, a = 0.f, b = 0.f;
-    if (i < Nu) {
-      const float sg = SG(i, sj), u1 = U1(i, sj), w1 = W1(i, sj);
-      const float s = g.S0[i] + sg;
-      const float iv = g.invVol[i];
-      ns = sg + dt * (fF[ri][sj] - fF[ri + 1][sj]) * iv;
-      float s2 = g.S0[i] + ns;
-      float d = (s2 < 1e-10f) ? 1e-10f : s2;
-      a = __fdividef(s * u1 + dt * (fFR[ri][sj] - fFR[ri + 1][sj]) * iv, d);
-      b = __fdividef(s * w1 + dt * (fGB[ri][sj] - fGA[ri + 1][sj]) * iv, d);
-    }
-    s2S[ri][sj] = ns; s2U[ri][sj] = a; s2W[ri][sj] = b;
-  }
-  __syncthreads();
-
-  // ---- transportPhi fluxes: face pj = j-1/2 of cell j0+pj ----
-  for (int c = tid; c < kTI32 * (kTJ32 + 1); c += kHydro32Threads) {
-    int ri = c / (kTJ32 + 1), pj = c % (kTJ32 + 1);
-    int i = i0 + ri;
-    float Fm = 0.f, FR = 0.f, G = 0.f;
-    if (i < Nu) {
-      const int cm = pj + 1, cc = pj + 2;
-      const float V = g.V0[i];
-      const float dv = 0.5f * (s2W[ri][cm] + s2W[ri][cc]);
-      const float vf = V + dv;
-      const int up = (vf > 0.f) ? cm : cc;
-      const float hf = (vf > 0.f) ? 0.5f * (1.f - vf * dt * g.invdl[i]) : -0.5f * (1.f + vf * dt * g.invdl[i]);
-      const float kS = vanleer32(s2S[ri][up + 1] - s2S[ri][up], s2S[ri][up] - s2S[ri][up - 1]);
-      const float kU = vanleer32(s2U[ri][up + 1] - s2U[ri][up], s2U[ri][up] - s2U[ri][up - 1]);
-      const float kW = vanleer32(s2W[ri][up + 1] - s2W[ri][up], s2W[ri][up] - s2W[ri][up - 1]);
-      const float sf = s2S[ri][up] + hf * kS;
-      const float Sf = g.S0[i] + sf;
-      const float uf = s2U[ri][up] + hf * kU;
-      const float wf = s2W[ri][up] + hf * kW;
-      const float A = g.Aphi[i];
-      const float Ffull = vf * Sf * A;
-      Fm = A * (V * sf + dv * Sf);
-      FR = Ffull * uf;
-      G = Ffull * wf;
-    }
-    pF[ri][pj] = Fm; pF[kTI32 + ri][pj] = FR; pF[2 * kTI32 + ri][pj] = G;
-  }
-  __syncthreads();
-
-  // ---- transportPhi gather + floor + outputs + next-step CFL ----
-  for (int c = tid; c < kTI32 * kTJ32; c += kHydro32Threads) {
-    int ri = c / kTJ32, pj = c % kTJ32;
-    int i = i0 + ri, j = j0 + pj;
-    if (i < Nu && j < Nphi) {
-      const int cc = pj + 2;
-      const float sg2 = s2S[ri][cc], u2 = s2U[ri][cc], w2 = s2W[ri][cc];
-      const float iv = g.invVol[i];
-      const float S0 = g.S0[i];
-      const float s2 = S0 + sg2;
-      float sg3 = sg2 + dt * (pF[ri][pj] - pF[ri][pj + 1]) * iv;
-      const float s3 = S0 + sg3;
-      const float d = (s3 < 1e-10f) ? 1e-10f : s3;
-      const float u3 = __fdividef(s2 * u2 + dt * (pF[kTI32 + ri][pj] - pF[kTI32 + ri][pj + 1]) * iv, d);
-      const float w3 = __fdividef(s2 * w2 + dt * (pF[2 * kTI32 + ri][pj] - pF[2 * kTI32 + ri][pj + 1]) * iv, d);
-      if (s3 < 1e-10f) sg3 = 1e-10f - S0;  // floor (hydro.hpp:69)
-      const size_t k = (size_t)i * Nphi + j;
-      so[k] = sg3; uo[k] = u3; wo[k] = w3;
-      const float x = g.R32[i] * sg3;
-      const __nv_bfloat16 hx = __float2bfloat16_rn(x);
-      Sx.hi[k] = hx;
-      Sx.lo[k] = __float2bfloat16_rn(x - __bfloat162float(hx));
-      const float rate = cfl_rate32(g, i, sg3, u3, w3);
-      bad |= !(rate == rate) || !(u3 == u3) || !(w3 == w3);
-      lmax = fmax(lmax, (double)rate);
-      if (nmodes) {
-        const double sfull = g.S0d[i] + (double)sg3;
-        const double phi = (j + 0.5) * (double)g.dphi;
-        for (int m = 0; m < nmodes; ++m) {
-          double sn, cs;
-          sincos(m * phi, &sn, &cs);
-          msum[2 * m] += sfull * cs * g.dAd[i];
-          msum[2 * m + 1] -= sfull * sn * g.dAd[i];
-        }
-      }
-    }
-  }
-  if (bad) lmax = __longlong_as_double(0x7ff8000000000000ll);
-  finish_launch<kHydro32Threads>(ctl, si, lmax, msum, red);
 }
 
 // CFL (and optional mode sums) over the perturbation state
@@ -766,6 +544,16 @@ int dg_handle::mixed_download_state(double *Sig, double *vRh, double *vph) {
   return DG_OK;
 }
 
+static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *u, const float *w, const float *Phi,
+                                  const double *gR, const double *gp, int fm, float *so, float *uo, float *wo, Ctl *ctl,
+                                  cudaStream_t st) {
+  const int nstrips = (X.Nphi + kOutCols32 - 1) / kOutCols32;
+  dim3 grid((nstrips + kWarps32 - 1) / kWarps32, (X.Nu + kBand32 - 1) / kBand32);
+  k_hydro32w<<<grid, kWarps32 * 32, 0, st>>>(sig, u, w, Phi, gR, gp, fm, so, uo, wo, SplitBf16{X.Sx.hi, X.Sx.lo}, ctl,
+                                             X.rows, nstrips);
+  return cudaGetLastError();
+}
+
 template <int MODE>
 static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUtensorMap &Bh, const CUtensorMap &Bl,
                         int M, int N, int K, const tc::GemmArgs &base, cudaStream_t st) {
@@ -808,11 +596,8 @@ int dg_handle::mixed_enqueue_step() {
     XK(prof_end(DG_PROF_GRAVITY));
     fm = kForcePhi;
   }
-  dim3 grid((p.Nphi + kTJ32 - 1) / kTJ32, (p.Nu + kTI32 - 1) / kTI32);
   XK(prof_begin(DG_PROF_HYDRO));
-  k_hydro32<<<grid, kHydro32Threads, 0, st>>>(X.sig[c], X.u[c], X.w[c], X.dPhi, nullptr, nullptr, fm, X.sig[o], X.u[o],
-                                              X.w[o], X.Sx, ctl, X.rows);
-  XK(cudaGetLastError());
+  XK(launch_hydro32(X, X.sig[c], X.u[c], X.w[c], X.dPhi, nullptr, nullptr, fm, X.sig[o], X.u[o], X.w[o], ctl, st));
   XK(prof_end(DG_PROF_HYDRO));
   cur = o;
   return DG_OK;
@@ -844,10 +629,7 @@ int dg_handle::mixed_enqueue_step_forces(const double *gRh, const double *gph) {
     fm = kForceArrays;
   }
   const int c = cur, o = cur ^ 1;
-  dim3 grid((p.Nphi + kTJ32 - 1) / kTJ32, (p.Nu + kTI32 - 1) / kTI32);
-  k_hydro32<<<grid, kHydro32Threads, 0, st>>>(X.sig[c], X.u[c], X.w[c], nullptr, gA, gB, fm, X.sig[o], X.u[o], X.w[o],
-                                              X.Sx, ctl, X.rows);
-  XK(cudaGetLastError());
+  XK(launch_hydro32(X, X.sig[c], X.u[c], X.w[c], nullptr, gA, gB, fm, X.sig[o], X.u[o], X.w[o], ctl, st));
   cur = o;
   return DG_OK;
 }
