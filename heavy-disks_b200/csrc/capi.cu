@@ -62,6 +62,7 @@ static int validate(const dg_params *p, std::string *why) {
   if (!(p->Kpoly > 0) || !(p->gamma_gas > 0)) { *why = "need Kpoly > 0 and gamma_gas > 0"; return DG_ERR_INVALID; }
   if (!(p->eps >= 0) || !std::isfinite(p->eps)) { *why = "need eps >= 0"; return DG_ERR_INVALID; }
   if (p->precision != DG_PREC_FP64 && p->precision != DG_PREC_MIXED) { *why = "precision must be DG_PREC_FP64 or DG_PREC_MIXED"; return DG_ERR_INVALID; }
+  if (p->basic_state != DG_BASIC_FFT && p->basic_state != DG_BASIC_ELLIPTIC) { *why = "basic_state must be DG_BASIC_FFT or DG_BASIC_ELLIPTIC"; return DG_ERR_INVALID; }
   FftPlan a, c;
   if (!make_fft_plan(p->Nphi, &a) || !make_fft_plan(2 * p->Nu, &c)) {
     snprintf(b, sizeof b, "Nphi=%d and 2*Nu=%d must factor into 2, 3 and 5", p->Nphi, 2 * p->Nu);
@@ -396,6 +397,7 @@ int dg_params_default(dg_params *p) {
   p->R0 = 0.45; p->w2 = 0.05; p->S0 = 0.372;
   p->precision = DG_PREC_FP64;
   p->device = -1;
+  p->basic_state = DG_BASIC_FFT;
   return DG_OK;
 }
 
@@ -493,7 +495,10 @@ int dg_init_standard(dg_handle *h) {
   const size_t n = (size_t)Nu * Nphi;
   auto Sigma0 = [&](double R) { return p.S0 * std::exp(-(R - p.R0) * (R - p.R0) / p.w2); };  // diskmain.cpp:34
   std::vector<double> gRdisk(Nu, 0.0);
-  if (p.selfgrav) {  // diskmain.cpp:37-48
+  if (p.selfgrav && p.basic_state == DG_BASIC_ELLIPTIC) {
+    int rc = dg_rotation_curve_elliptic(&p, Nu, h->R.data(), gRdisk.data(), nullptr, nullptr, nullptr);
+    if (rc) return h->fail(rc, "dg_init_standard", "elliptic rotation curve");
+  } else if (p.selfgrav) {  // diskmain.cpp:37-48
     std::vector<double> Sig_axi(n), gR_eq(n);
     for (int i = 0; i < Nu; ++i)
       for (int j = 0; j < Nphi; ++j) Sig_axi[(size_t)i * Nphi + j] = Sigma0(h->R[i]);

@@ -44,7 +44,7 @@ class Params(C.Structure):
         ("Kpoly", C.c_double), ("gamma_gas", C.c_double), ("gmstar", C.c_double), ("G", C.c_double),
         ("eps", C.c_double), ("selfgrav", C.c_int), ("amp", C.c_double), ("phase0", C.c_double),
         ("R0", C.c_double), ("w2", C.c_double), ("S0", C.c_double),
-        ("precision", C.c_int), ("device", C.c_int),
+        ("precision", C.c_int), ("device", C.c_int), ("basic_state", C.c_int),
     ]
 
 
@@ -58,8 +58,10 @@ EXPORTS = (
     "dg_init_standard", "dg_set_state", "dg_get_state", "dg_timestep", "dg_step", "dg_step_forces",
     "dg_potential", "dg_forces", "dg_disk_mass", "dg_modes", "dg_conserved", "dg_advance", "dg_time",
     "dg_set_stream", "dg_run_steps", "dg_step_host", "dg_profile_enable", "dg_profile_read",
-    "dg_timestep_static",
+    "dg_timestep_static", "dg_rotation_curve_elliptic", "dg_params_physical",
 )
+
+BASIC_FFT, BASIC_ELLIPTIC = 0, 1
 
 PROF_HYDRO, PROF_GRAVITY, PROF_CFL, PROF_N = 0, 1, 2, 3
 
@@ -105,6 +107,8 @@ def lib():
     L.dg_step_host.argtypes = [H, C.c_double, D, D, D, D]
     L.dg_profile_enable.argtypes = [H, C.c_int]
     L.dg_profile_read.argtypes = [H, D, C.POINTER(C.c_longlong)]
+    L.dg_rotation_curve_elliptic.argtypes = [C.POINTER(Params), C.c_int, D, D, D, D, D]
+    L.dg_params_physical.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(Params), D]
     L.dg_timestep_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double,
                                      C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     _lib = L
@@ -128,15 +132,46 @@ def default_params(**kw) -> Params:
     for k, v in kw.items():
         if k == "precision" and isinstance(v, str):
             v = {"fp64": FP64, "mixed": MIXED}[v]
+        if k == "basic_state" and isinstance(v, str):
+            v = {"fft": BASIC_FFT, "elliptic": BASIC_ELLIPTIC}[v]
         setattr(p, k, v)
     return p
+
+
+def rotation_curve_elliptic(R, **kw):
+    """FP64 elliptic-integral basic state at radii R: dict of gR, vphi2, kappa2, Q."""
+    p = default_params(**kw)
+    R = np.ascontiguousarray(R, dtype=np.float64)
+    out = {k: np.empty_like(R) for k in ("gR", "vphi2", "kappa2", "Q")}
+    rc = lib().dg_rotation_curve_elliptic(C.byref(p), len(R), _dp(R), _dp(out["gR"]), _dp(out["vphi2"]),
+                                          _dp(out["kappa2"]), _dp(out["Q"]))
+    if rc != DG_OK:
+        raise DiskGPUError(rc, "dg_rotation_curve_elliptic")
+    return out
+
+
+def params_physical(Qmin, mass_ratio, soft_over_r, gamma_gas, **kw):
+    """(dg_params, achieved Q_min) for a sweep point (Q_min, M_d/M_*, softening/r, Gamma)."""
+    p = default_params(**kw)
+    q = C.c_double()
+    rc = lib().dg_params_physical(Qmin, mass_ratio, soft_over_r, gamma_gas, C.byref(p), C.byref(q))
+    if rc != DG_OK:
+        raise DiskGPUError(rc, "dg_params_physical")
+    return p, q.value
 
 
 class Disk:
     """One disk on one GPU: the handle of include/diskgpu.h."""
 
-    def __init__(self, Nu=128, Nphi=128, eps=0.02, selfgrav=1, amp=1e-3, precision="fp64", **kw):
-        self.p = default_params(Nu=Nu, Nphi=Nphi, eps=eps, selfgrav=selfgrav, amp=amp, precision=precision, **kw)
+    def __init__(self, Nu=128, Nphi=128, eps=0.02, selfgrav=1, amp=1e-3, precision="fp64", params=None, **kw):
+        if params is not None:
+            self.p = Params.from_buffer_copy(params)
+            for k, v in dict(Nu=Nu, Nphi=Nphi, precision=precision, amp=amp, **kw).items():
+                if k == "precision" and isinstance(v, str):
+                    v = {"fp64": FP64, "mixed": MIXED}[v]
+                setattr(self.p, k, v)
+        else:
+            self.p = default_params(Nu=Nu, Nphi=Nphi, eps=eps, selfgrav=selfgrav, amp=amp, precision=precision, **kw)
         self.Nu, self.Nphi = Nu, Nphi
         h = C.c_void_p()
         rc = lib().dg_create(C.byref(self.p), C.byref(h))

@@ -62,7 +62,12 @@ typedef struct dg_params {
   double R0, w2, S0;     /* Gaussian disk Sigma0 = S0 exp(-(R-R0)^2/w2) (0.45, 0.05, 0.372) */
   int precision;         /* DG_PREC_FP64 or DG_PREC_MIXED */
   int device;            /* CUDA device ordinal; -1 = the calling thread's current device */
+  int basic_state;       /* rotation curve of dg_init_standard: DG_BASIC_FFT (the reference's,
+                            diskmain.cpp:41-56) or DG_BASIC_ELLIPTIC (complete elliptic integrals) */
 } dg_params;
+
+#define DG_BASIC_FFT 0
+#define DG_BASIC_ELLIPTIC 1
 
 /* One row of the mode table: diskmain.cpp:93-97 prints t, |C0|, |C2|, arg(C2). */
 typedef struct dg_record {
@@ -127,6 +132,23 @@ int dg_advance(dg_handle *h, double tlim, double cfl, double dtout, dg_record *r
                int *n_rec, double *t, long long *nsteps);
 /* Simulation time and step count of the handle. */
 int dg_time(dg_handle *h, double *t, long long *nsteps);
+
+/* ---- FP64 host-side basic state (no device work) ---- */
+
+/* Disk self-gravity force gR(R) (negative inward), vphi^2, kappa^2 and Toomre Q at radii
+ * R[0..n) (increasing), from complete elliptic integrals with the Kalnajs kernel's
+ * softening eps R R'.  It is the closed form of lka98/selfgravity.py:35-95 with that
+ * softening; vphi^2 follows diskmain.cpp:55.  Any output pointer may be NULL. */
+int dg_rotation_curve_elliptic(const dg_params *p, int n, const double *R, double *gR, double *vphi2,
+                               double *kappa2, double *Q);
+/* Map sweep parameters onto *p (other fields kept): eps = soft_over_r^2, gamma_gas, S0 so
+ * that the disk mass is mass_ratio * M_* (G M_* = p->gmstar), and Kpoly so that the minimum
+ * of the elliptic-integral Toomre Q (defined as in lka98/selfgravity.py:98-102) over the disk
+ * body (Sigma0 >= 0.1 S0) equals Qmin.  K is capped at the largest value for which the
+ * equilibrium exists over the body (vphi^2 > 0, kappa^2 > 0); *Qmin_achieved (may be NULL)
+ * receives the minimum Q actually reached, which is below Qmin when the cap binds. */
+int dg_params_physical(double Qmin, double mass_ratio, double soft_over_r, double gamma_gas, dg_params *p,
+                       double *Qmin_achieved);
 
 /* ---- GPU-side extensions (no counterpart in the CPU reference) ---- */
 
