@@ -26,16 +26,20 @@ def test_disk_force_matches_scipy(R, eps):
 
 
 def test_elliptic_vs_fft_equilibrium_stated_error():
-    """The two basic states differ by the discretisation of the FFT solver (O(du^2))."""
-    errs = []
-    for N in (128, 256):
-        d = O.Disk(Nu=N, Nphi=32, eps=0.005, amp=0.0)
+    """The two basic states differ by the FFT solver's discretisation: the median error
+    falls as N^-2 (6e-5 at 64^2, 2e-5 at 128^2) and the maximum, set by the one-sided
+    force differences at the outer edge, as N^-1 (4.6e-3, 2.3e-3)."""
+    med, mx = [], []
+    for N in (64, 128):
+        d = O.Disk(Nu=N, Nphi=N, eps=0.005, amp=0.0, nthreads=4)
         R = d.hyd.get("R")
         vf = d.hyd.get("vp")[:, 0]
         ve = np.sqrt(D.rotation_curve_elliptic(R, eps=0.005)["vphi2"])
-        errs.append(np.max(np.abs(ve - vf) / vf))
-    assert errs[1] < 2e-3
-    assert errs[1] < errs[0]  # converges with resolution
+        e = np.abs(ve - vf) / vf
+        med.append(np.median(e))
+        mx.append(e.max())
+    assert mx[1] < 3e-3 and med[1] < 3e-5
+    assert med[1] < 0.5 * med[0] and mx[1] < 0.6 * mx[0]
 
 
 @pytest.mark.parametrize("args", [(1.0, 0.2, 0.1, 1.8), (1.5, 0.2, 0.1, 1.8), (1.0, 0.5, 0.1, 1.8),
