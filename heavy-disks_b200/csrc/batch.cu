@@ -1,0 +1,216 @@
+// Batched sweeps: many independent disks (heterogeneous grids and parameters) advanced
+// together by one CUDA graph per launch.  The graph forks one branch per disk from a
+// root stream; each branch holds that disk's steps (gravity + hydro kernels) on the disk's
+// own stream, so the disks' kernels overlap on the GPU, and joins back.  Every disk keeps
+// its own device-resident dt, time and record ring (dg::Ctl); a disk that reaches tlim
+// turns the rest of its branch into pass-through launches.  Disks with a smaller dt get
+// proportionally more steps per launch so that the branches finish together.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+struct dg_batch {
+  std::vector<dg_handle *> disks;
+  std::vector<int> steps_per_launch;
+  cudaStream_t root = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<cudaEvent_t> events;
+  int dev = -1;
+  std::string err;
+  int fail(int code, const char *what, const char *why) {
+    err = std::string(what) + ": " + (why ? why : "");
+    return code;
+  }
+  void release_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+  }
+};
+
+#define BK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) return b->fail(DG_ERR_CUDA, #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+extern "C" {
+
+int dg_batch_create(int n, const dg_params *params, dg_batch **out) {
+  if (n < 1 || !params || !out) return DG_ERR_INVALID;
+  *out = nullptr;
+  dg_batch *b = new (std::nothrow) dg_batch();
+  if (!b) return DG_ERR_NOMEM;
+  for (int k = 0; k < n; ++k) {
+    if (k > 0 && params[k].device != params[0].device) {
+      delete b;
+      return DG_ERR_INVALID;
+    }
+    dg_handle *h = nullptr;
+    int rc = dg_create(&params[k], &h);
+    if (rc) {
+      for (dg_handle *d : b->disks) dg_destroy(d);
+      delete b;
+      return rc;
+    }
+    b->disks.push_back(h);
+  }
+  b->dev = b->disks[0]->dev;
+  cudaSetDevice(b->dev);
+  if (cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking) != cudaSuccess) {
+    for (dg_handle *d : b->disks) dg_destroy(d);
+    delete b;
+    return DG_ERR_CUDA;
+  }
+  b->events.resize(n + 1);
+  for (auto &e : b->events) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  *out = b;
+  return DG_OK;
+}
+
+void dg_batch_destroy(dg_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->dev);
+  if (b->root) cudaStreamSynchronize(b->root);
+  b->release_graph();
+  for (auto &e : b->events) cudaEventDestroy(e);
+  for (dg_handle *d : b->disks) dg_destroy(d);
+  if (b->root) cudaStreamDestroy(b->root);
+  delete b;
+}
+
+const char *dg_batch_last_error(const dg_batch *b) { return b ? b->err.c_str() : ""; }
+
+int dg_batch_size(const dg_batch *b) { return b ? (int)b->disks.size() : 0; }
+
+dg_handle *dg_batch_disk(dg_batch *b, int k) {
+  if (!b || k < 0 || k >= (int)b->disks.size()) return nullptr;
+  return b->disks[k];
+}
+
+int dg_batch_init_standard(dg_batch *b) {
+  if (!b) return DG_ERR_INVALID;
+  for (dg_handle *h : b->disks) {
+    int rc = dg_init_standard(h);
+    if (rc) return b->fail(rc, "dg_batch_init_standard", dg_last_error(h));
+  }
+  b->release_graph();
+  return DG_OK;
+}
+
+int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int steps_per_launch, dg_record *rec,
+                     int max_rec_per_disk, int *n_rec, double *t_out, long long *nsteps_out) {
+  if (!b || !(cfl > 0) || !(dtout > 0) || steps_per_launch < 2 || (max_rec_per_disk > 0 && !rec)) return DG_ERR_INVALID;
+  BK(cudaSetDevice(b->dev));
+  const int n = (int)b->disks.size();
+  std::vector<int> nout(n, 0);
+  // per-disk loop set-up, as dg_advance does for one disk
+  for (int k = 0; k < n; ++k) {
+    dg_handle *h = b->disks[k];
+    if (!h->have_state) return b->fail(DG_ERR_STATE, "dg_batch_advance", "a disk has no state");
+    int rc = h->sync_from_device();
+    if (rc) return b->fail(rc, "dg_batch_advance", h->err.c_str());
+    if (h->cur != 0) {  // the graph assumes every disk starts on ping-pong buffer 0
+      rc = h->set_ctl_fields(h->t, tlim, cfl, 0.0, h->tnext, dtout, 0);
+      if (!rc) rc = h->cfl_launch(0, 0);
+      if (!rc) rc = h->run_chunk(1);
+      if (!rc) rc = h->read_ctl();
+      if (rc) return b->fail(rc, "dg_batch_advance", h->err.c_str());
+      h->t = h->hctl->t;
+      h->nsteps = h->hctl->step;
+    }
+    rc = h->set_ctl_fields(h->t, tlim, cfl, 0.0, h->tnext, dtout, 0);
+    if (rc) return b->fail(rc, "dg_batch_advance", h->err.c_str());
+    BK(cudaMemsetAsync(&h->ctl->nrec, 0, sizeof(int), h->st));
+    const bool first = (h->t < tlim) && (h->t >= h->tnext - 1e-12);
+    rc = h->cfl_launch(0, first ? 1 : 0);
+    if (rc) return b->fail(rc, "dg_batch_advance", h->err.c_str());
+    rc = h->read_ctl();
+    if (rc) return b->fail(rc, "dg_batch_advance", h->err.c_str());
+  }
+  // steps per launch: proportional to each disk's step rate (1/dt), even, at least 2
+  if (!b->exec) {
+    double dtmin = 1e300;
+    for (dg_handle *h : b->disks) dtmin = std::min(dtmin, h->hctl->dt > 0 ? h->hctl->dt : 1e300);
+    b->steps_per_launch.assign(n, steps_per_launch);
+    double dtmax = 0;
+    for (dg_handle *h : b->disks) dtmax = std::max(dtmax, h->hctl->dt);
+    for (int k = 0; k < n; ++k) {
+      double ratio = (b->disks[k]->hctl->dt > 0) ? dtmin / b->disks[k]->hctl->dt : 1.0;
+      int s = (int)std::lround(steps_per_launch * ratio);
+      s = std::max(2, s + (s & 1));
+      b->steps_per_launch[k] = s;
+    }
+    // capture: root -> fork to every disk stream -> K_k steps each -> join
+    for (dg_handle *h : b->disks) {
+      int rc0 = h->prof_collect();
+      if (rc0) return b->fail(rc0, "dg_batch_advance", h->err.c_str());
+      h->prof_on = false;  // no event timing inside the batch graph
+    }
+    cudaGraph_t g = nullptr;
+    BK(cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecord(b->events[n], b->root);
+    int rc = DG_OK;
+    for (int k = 0; k < n && !rc; ++k) {
+      dg_handle *h = b->disks[k];
+      cudaStreamWaitEvent(h->st, b->events[n], 0);
+      for (int s = 0; s < b->steps_per_launch[k] && !rc; ++s) rc = h->enqueue_step();
+      cudaEventRecord(b->events[k], h->st);
+      cudaStreamWaitEvent(b->root, b->events[k], 0);
+    }
+    cudaError_t e = cudaStreamEndCapture(b->root, &g);
+    for (dg_handle *h : b->disks) h->cur = 0;  // capture flipped the buffers an even number of times
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return b->fail(rc, "dg_batch_advance", "capture");
+    }
+    BK(e);
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    cudaGraphDestroy(g);
+    BK(e);
+  }
+  std::vector<double> tmp;
+  for (;;) {
+    // read every control block with one synchronisation
+    for (dg_handle *h : b->disks)
+      BK(cudaMemcpyAsync(h->hctl, h->ctl, offsetof(dg::Ctl, rec), cudaMemcpyDeviceToHost, b->root));
+    BK(cudaStreamSynchronize(b->root));
+    bool running = false;
+    for (int k = 0; k < n; ++k) {
+      dg_handle *h = b->disks[k];
+      const int nr = h->hctl->nrec;
+      if (nr > 0) {
+        tmp.resize((size_t)nr * 4);
+        BK(cudaMemcpy(tmp.data(), &h->ctl->rec[0][0], (size_t)nr * 4 * sizeof(double), cudaMemcpyDeviceToHost));
+        BK(cudaMemset(&h->ctl->nrec, 0, sizeof(int)));
+        for (int q = 0; q < nr; ++q) {
+          if (nout[k] < max_rec_per_disk) {
+            dg_record &r = rec[(size_t)k * max_rec_per_disk + nout[k]];
+            r.t = tmp[4 * q]; r.c0 = tmp[4 * q + 1]; r.c2 = tmp[4 * q + 2]; r.arg2 = tmp[4 * q + 3];
+          }
+          ++nout[k];
+        }
+      }
+      h->t = h->hctl->t;
+      h->nsteps = h->hctl->step;
+      int rc = h->check_status();
+      if (rc) return b->fail(rc, "dg_batch_advance", h->err.c_str());
+      if (h->t < tlim) running = true;
+    }
+    if (!running) break;
+    BK(cudaGraphLaunch(b->exec, b->root));
+  }
+  for (int k = 0; k < n; ++k) {
+    dg_handle *h = b->disks[k];
+    h->tnext = h->hctl->tnext;
+    if (n_rec) n_rec[k] = std::min(nout[k], max_rec_per_disk);
+    if (t_out) t_out[k] = h->t;
+    if (nsteps_out) nsteps_out[k] = h->nsteps;
+  }
+  return DG_OK;
+}
+
+}  // extern "C"

@@ -176,6 +176,7 @@ void dg_handle::release() {
   if (st) cudaStreamSynchronize(st);
   mixed_release();
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (diag) cudaFree(diag);
   void *ptrs[] = {rowtab, dR, dRf, dVol, dSqrtR, dR32, S[0], S[1], VR[0], VR[1], VP[0], VP[1], dPhi, gA, gB,
                   W, Khat, rootsPhi, rootsM, scratch, ctl};
   for (void *q : ptrs)

@@ -36,7 +36,10 @@ struct Ctl {
   int status;                      // kSt* bits
   long long step;                  // completed steps
   int nrec;                        // records written since the last host drain
-  int pad1;
+  int ndiag;                       // per-step diagnostic rows written since the last drain
+  double *diag;                    // per-step diagnostic ring (host-allocated on request), or null
+  int diag_cap;                    // rows the ring holds
+  int pad2;
   double modesum[2 * kMaxModes];   // re/im sums for the record being built
   double last_modes[2 * kMaxModes];// the most recent per-step sums (mode_every_step)
   double rec[kMaxRecords][4];      // t, |C0|, |C2|, arg C2

@@ -96,4 +96,13 @@ struct dg_handle {
   int mixed_gravity();
   int mixed_potential(const double *dSig, double *dOut);
   bool in_step_host = false;  // upload from dg_step_host keeps the mixed basic state
+  void mixed_basic(std::vector<double> *S0, std::vector<double> *V0, std::vector<double> *g0) const;
+
+  // per-step diagnostic ring (dg_set_diagnostics)
+  double *diag = nullptr;
+  int diag_mmax = 0;
+  void graph_reset() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+  }
 };

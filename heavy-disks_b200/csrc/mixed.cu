@@ -390,6 +390,16 @@ int dg_handle::mixed_init() {
   return DG_OK;
 }
 
+void dg_handle::mixed_basic(std::vector<double> *S0, std::vector<double> *V0, std::vector<double> *g0) const {
+  if (!mx) {
+    S0->clear(); V0->clear(); g0->clear();
+    return;
+  }
+  *S0 = mx->S0;
+  *V0 = mx->V0;
+  *g0 = mx->g0;
+}
+
 void dg_handle::mixed_release() {
   if (!mx) return;
   MixedState &X = *mx;

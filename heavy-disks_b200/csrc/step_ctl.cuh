@@ -91,6 +91,14 @@ __device__ __forceinline__ void finish_launch(Ctl *ctl, const StepInfo &si, doub
       }
       ctl->tnext += ctl->dtout;
     }
+    // per-step diagnostic row: t, then Re/Im of sum Sigma e^{-i m phi} dA for m = 0..mmax
+    if (ctl->mode_every_step && si.active && si.advance_t && ctl->diag && ctl->ndiag < ctl->diag_cap) {
+      const int w = 1 + 2 * (ctl->mmax + 1);
+      double *row = ctl->diag + (size_t)ctl->ndiag * w;
+      row[0] = t;
+      for (int q = 0; q < 2 * (ctl->mmax + 1); ++q) row[1 + q] = ctl->modesum[q];
+      ctl->ndiag += 1;
+    }
     for (int q = 0; q < 2 * kMaxModes; ++q) ctl->modesum[q] = 0.0;
   }
   ctl->dtinv_bits = 0ull;

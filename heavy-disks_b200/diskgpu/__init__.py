@@ -59,6 +59,9 @@ EXPORTS = (
     "dg_potential", "dg_forces", "dg_disk_mass", "dg_modes", "dg_conserved", "dg_advance", "dg_time",
     "dg_set_stream", "dg_run_steps", "dg_step_host", "dg_profile_enable", "dg_profile_read",
     "dg_timestep_static", "dg_rotation_curve_elliptic", "dg_params_physical",
+    "dg_batch_create", "dg_batch_destroy", "dg_batch_last_error", "dg_batch_size", "dg_batch_disk",
+    "dg_batch_init_standard", "dg_batch_advance", "dg_save", "dg_load", "dg_set_diagnostics",
+    "dg_diagnostics_read",
 )
 
 BASIC_FFT, BASIC_ELLIPTIC = 0, 1
@@ -109,6 +112,21 @@ def lib():
     L.dg_profile_read.argtypes = [H, D, C.POINTER(C.c_longlong)]
     L.dg_rotation_curve_elliptic.argtypes = [C.POINTER(Params), C.c_int, D, D, D, D, D]
     L.dg_params_physical.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(Params), D]
+    L.dg_batch_create.argtypes = [C.c_int, C.POINTER(Params), C.POINTER(H)]
+    L.dg_batch_destroy.argtypes = [H]
+    L.dg_batch_destroy.restype = None
+    L.dg_batch_last_error.argtypes = [H]
+    L.dg_batch_last_error.restype = C.c_char_p
+    L.dg_batch_size.argtypes = [H]
+    L.dg_batch_disk.argtypes = [H, C.c_int]
+    L.dg_batch_disk.restype = H
+    L.dg_batch_init_standard.argtypes = [H]
+    L.dg_batch_advance.argtypes = [H, C.c_double, C.c_double, C.c_double, C.c_int, C.POINTER(Record), C.c_int,
+                                   C.POINTER(C.c_int), D, C.POINTER(C.c_longlong)]
+    L.dg_save.argtypes = [H, C.c_char_p]
+    L.dg_load.argtypes = [H, C.c_char_p]
+    L.dg_set_diagnostics.argtypes = [H, C.c_int, C.c_int]
+    L.dg_diagnostics_read.argtypes = [H, D, C.c_int, C.POINTER(C.c_int)]
     L.dg_timestep_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double,
                                      C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     _lib = L
@@ -287,6 +305,27 @@ class Disk:
         return out, t.value, s.value
 
 
+    def save(self, path):
+        self._ck(lib().dg_save(self.h, os.fsencode(path)))
+
+    def load(self, path):
+        self._ck(lib().dg_load(self.h, os.fsencode(path)))
+
+    def set_diagnostics(self, mmax=8, capacity=4096):
+        """Record C_0..C_mmax on the device every step (capacity 0 = off)."""
+        self._ck(lib().dg_set_diagnostics(self.h, mmax, capacity))
+        self._diag_mmax = mmax
+
+    def diagnostics(self, max_rows=1 << 20):
+        """Drain the per-step ring: (t[n], C[n, mmax+1] complex)."""
+        mm = getattr(self, "_diag_mmax", 8)
+        w = 1 + 2 * (mm + 1)
+        buf = np.empty(max_rows * w)
+        n = C.c_int()
+        self._ck(lib().dg_diagnostics_read(self.h, _dp(buf), max_rows, C.byref(n)))
+        rows = buf[: n.value * w].reshape(n.value, w)
+        return rows[:, 0].copy(), rows[:, 1::2] + 1j * rows[:, 2::2]
+
     # ---- GPU-side extensions ----
     def set_stream(self, stream_ptr):
         """Queue all work of this disk on a caller CUDA stream (int handle; 0 = own stream)."""
@@ -315,6 +354,79 @@ class Disk:
         self._ck(lib().dg_profile_read(self.h, _dp(ms), cnt))
         names = ("hydro", "gravity", "cfl")
         return {names[k]: (float(ms[k]), int(cnt[k])) for k in range(PROF_N)}
+
+
+class _BorrowedDisk(Disk):
+    """A disk owned by a Batch (no destroy on close)."""
+
+    def __init__(self, handle, params):
+        self.h = handle
+        self.p = params
+        self.Nu, self.Nphi = params.Nu, params.Nphi
+        self.R = np.empty(self.Nu)
+        self.Rf = np.empty(self.Nu + 1)
+        self.Vol = np.empty(self.Nu)
+        self._ck(lib().dg_grid(self.h, _dp(self.R), _dp(self.Rf), _dp(self.Vol)))
+        self.dphi = 2.0 * np.pi / self.Nphi
+
+    def close(self):
+        self.h = None
+
+
+class Batch:
+    """Many independent disks advanced by one CUDA graph per launch (dg_batch)."""
+
+    def __init__(self, params_list):
+        arr = (Params * len(params_list))(*[Params.from_buffer_copy(p) for p in params_list])
+        h = C.c_void_p()
+        rc = lib().dg_batch_create(len(params_list), arr, C.byref(h))
+        if rc != DG_OK:
+            raise DiskGPUError(rc, lib().dg_last_error(None).decode())
+        self.h = h
+        self.n = len(params_list)
+        self.disks = [_BorrowedDisk(lib().dg_batch_disk(h, k), Params.from_buffer_copy(params_list[k]))
+                      for k in range(self.n)]
+
+    def _ck(self, rc):
+        if rc != DG_OK:
+            raise DiskGPUError(rc, lib().dg_batch_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            for d in self.disks:
+                d.close()
+            lib().dg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def init_standard(self):
+        self._ck(lib().dg_batch_init_standard(self.h))
+
+    def advance(self, tlim, cfl=0.3, dtout=0.25, steps_per_launch=16, max_rec=None):
+        """Advance all disks to tlim; returns (list of (n_k, 4) record arrays, t[n], steps[n])."""
+        if max_rec is None:
+            max_rec = int(tlim / dtout) + 8
+        recs = (Record * (self.n * max_rec))()
+        nrec = (C.c_int * self.n)()
+        t = np.zeros(self.n)
+        s = (C.c_longlong * self.n)()
+        self._ck(lib().dg_batch_advance(self.h, tlim, cfl, dtout, steps_per_launch, recs, max_rec, nrec, _dp(t), s))
+        out = []
+        for k in range(self.n):
+            rr = recs[k * max_rec: k * max_rec + nrec[k]]
+            out.append(np.array([[r.t, r.c0, r.c2, r.arg2] for r in rr]).reshape(-1, 4))
+        return out, t, np.array(list(s))
 
 
 class DiskHydro:

@@ -133,6 +133,41 @@ int dg_advance(dg_handle *h, double tlim, double cfl, double dtout, dg_record *r
 /* Simulation time and step count of the handle. */
 int dg_time(dg_handle *h, double *t, long long *nsteps);
 
+/* Snapshot / restart (new: the reference keeps its state only in the process).  The file
+ * holds the parameters, t, the next record time, m_D, the step count, the full FP64
+ * fields and, for the mixed path, its basic state, so a restarted run continues bit for
+ * bit.  dg_load needs a handle with the same grid, precision and physics parameters. */
+int dg_save(dg_handle *h, const char *path);
+int dg_load(dg_handle *h, const char *path);
+
+/* Per-step Fourier diagnostics on the device (m = 0..mmax, mmax <= 8): with capacity > 0
+ * every device step appends a row (t, Re C_0, Im C_0, ..., Re C_mmax, Im C_mmax) to a
+ * ring of `capacity` rows; C_m is normalised by m_D as in diskmain.cpp:72-84.  capacity 0
+ * turns it off.  dg_diagnostics_read copies up to max_rows rows (oldest first), sets *n
+ * and empties the ring; rows written while the ring is full are dropped. */
+int dg_set_diagnostics(dg_handle *h, int mmax, int capacity);
+int dg_diagnostics_read(dg_handle *h, double *rows, int max_rows, int *n);
+
+/* ---- Batched sweeps: many independent disks in one graph launch ---- */
+
+typedef struct dg_batch dg_batch;
+/* n disks (heterogeneous grids / parameters, one device) advanced together: each launch is
+ * one CUDA graph with one branch per disk, each branch holding that disk's steps on its
+ * own stream.  The disks are ordinary handles (dg_batch_disk) for state and diagnostics. */
+int dg_batch_create(int n, const dg_params *params, dg_batch **out);
+void dg_batch_destroy(dg_batch *b);
+const char *dg_batch_last_error(const dg_batch *b);
+int dg_batch_size(const dg_batch *b);
+/* Borrowed handle of disk k (owned by the batch; do not destroy). */
+dg_handle *dg_batch_disk(dg_batch *b, int k);
+int dg_batch_init_standard(dg_batch *b);
+/* dg_advance for every disk to the same tlim.  Each graph launch runs about
+ * steps_per_launch steps of the disk with the smallest dt and proportionally more of the
+ * others.  rec holds n * max_rec_per_disk records (disk k at k * max_rec_per_disk);
+ * n_rec, t and nsteps receive n values each (any may be NULL). */
+int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int steps_per_launch, dg_record *rec,
+                     int max_rec_per_disk, int *n_rec, double *t, long long *nsteps);
+
 /* ---- FP64 host-side basic state (no device work) ---- */
 
 /* Disk self-gravity force gR(R) (negative inward), vphi^2, kappa^2 and Toomre Q at radii
