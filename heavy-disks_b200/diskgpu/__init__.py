@@ -61,7 +61,8 @@ EXPORTS = (
     "dg_timestep_static", "dg_rotation_curve_elliptic", "dg_params_physical",
     "dg_batch_create", "dg_batch_destroy", "dg_batch_last_error", "dg_batch_size", "dg_batch_disk",
     "dg_batch_init_standard", "dg_batch_advance", "dg_save", "dg_load", "dg_set_diagnostics",
-    "dg_diagnostics_read",
+    "dg_diagnostics_read", "dg_mlp_create", "dg_mlp_destroy", "dg_mlp_last_error", "dg_mlp_num_params",
+    "dg_mlp_get_params", "dg_mlp_set_params", "dg_mlp_forward", "dg_mlp_loss_grad", "dg_mlp_train_step",
 )
 
 BASIC_FFT, BASIC_ELLIPTIC = 0, 1
@@ -127,6 +128,19 @@ def lib():
     L.dg_load.argtypes = [H, C.c_char_p]
     L.dg_set_diagnostics.argtypes = [H, C.c_int, C.c_int]
     L.dg_diagnostics_read.argtypes = [H, D, C.c_int, C.POINTER(C.c_int)]
+    Fp = C.POINTER(C.c_float)
+    L.dg_mlp_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.c_int, C.POINTER(H)]
+    L.dg_mlp_destroy.argtypes = [H]
+    L.dg_mlp_destroy.restype = None
+    L.dg_mlp_last_error.argtypes = [H]
+    L.dg_mlp_last_error.restype = C.c_char_p
+    L.dg_mlp_num_params.argtypes = [H]
+    L.dg_mlp_num_params.restype = C.c_longlong
+    L.dg_mlp_get_params.argtypes = [H, Fp]
+    L.dg_mlp_set_params.argtypes = [H, Fp]
+    L.dg_mlp_forward.argtypes = [H, C.c_int, Fp, Fp]
+    L.dg_mlp_loss_grad.argtypes = [H, C.c_int, Fp, Fp, Fp, Fp]
+    L.dg_mlp_train_step.argtypes = [H, C.c_int, Fp, Fp, C.c_float, Fp]
     L.dg_timestep_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double,
                                      C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     _lib = L

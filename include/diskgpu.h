@@ -168,6 +168,27 @@ int dg_batch_init_standard(dg_batch *b);
 int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int steps_per_launch, dg_record *rec,
                      int max_rec_per_disk, int *n_rec, double *t, long long *nsteps);
 
+/* ---- Learned surrogate (no counterpart in the reference) ---- */
+
+typedef struct dg_mlp dg_mlp;
+/* MLP n_in -> depth hidden layers of `width` (SiLU) -> n_out (linear), trained and run by
+ * the library's own CUDA kernels: BF16 weights in every product, FP32 activations and
+ * accumulation, FP32 master weights updated by Adam.  Parameters are one flat FP32 vector,
+ * per layer W (fan_out x fan_in, row-major) then b.  Host buffers, row-major samples. */
+int dg_mlp_create(int n_in, int width, int depth, int n_out, unsigned long long seed, int device, dg_mlp **out);
+void dg_mlp_destroy(dg_mlp *m);
+const char *dg_mlp_last_error(const dg_mlp *m);
+long long dg_mlp_num_params(const dg_mlp *m);
+int dg_mlp_get_params(dg_mlp *m, float *params);
+/* Also resets the Adam state. */
+int dg_mlp_set_params(dg_mlp *m, const float *params);
+int dg_mlp_forward(dg_mlp *m, int n, const float *x, float *y);
+/* Mean-squared-error loss over n samples and its gradient w.r.t. the parameters (grad may
+ * be NULL). */
+int dg_mlp_loss_grad(dg_mlp *m, int n, const float *x, const float *t, float *loss, float *grad);
+/* One Adam step (beta 0.9 / 0.999) on the batch; *loss receives the loss before the step. */
+int dg_mlp_train_step(dg_mlp *m, int n, const float *x, const float *t, float lr, float *loss);
+
 /* ---- FP64 host-side basic state (no device work) ---- */
 
 /* Disk self-gravity force gR(R) (negative inward), vphi^2, kappa^2 and Toomre Q at radii
