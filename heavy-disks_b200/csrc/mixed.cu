@@ -2,8 +2,9 @@
 // gravity of the perturbation as a split-BF16 tensor-core DFT (four tcgen05 GEMMs).
 //
 // Gravity (kalnajs.hpp:48-63 restated as dense real DFT contractions; s = R^{3/2} sigma):
-//   G1  X[c][i]  = sum_j Fphi[c][j] s[i][j]     phi DFT, c in [0, Nphi): Re m=0..Nphi/2,
-//                                               Im m=1..ceil(Nphi/2)-1 (the other Im are 0)
+//   G1  X[c][i]  = sum_j Fphi[c][j] s[i][j]     phi DFT, c in [0, Nphi): Re m = 0, Re m = Nphi/2,
+//                                               then (Re, Im) of m = 1..Nphi/2-1 interleaved
+//                                               (the other imaginary parts vanish)
 //   G2  W[c][p]  = KW[c][p] sum_i Cu[p][i] X[c][i]
 //                                               u DFT on 2 Nu rows (cos p=0..Nu, sin p=1..Nu-1)
 //                                               times (w_p / M) khat(p, m(c)) (khat is real and
@@ -47,6 +48,13 @@ struct MixedState {
   SplitBuf Sx, X1, Wt, Z, Fphi, Cu, CuT, Gphi;
   float *KW = nullptr, *dPhi = nullptr, *phiscale = nullptr;
   CUtensorMap mFphi[2], mSx[2], mX1[2], mCu[2], mCuT[2], mWt[2], mZ[2], mGphi[2];
+  // factored u-direction (Nu a multiple of 1024): M = 2 Nu = 64 A, A = Nu / 32
+  bool factored = false;
+  int fa = 0, nm = 0;  // A and the padded complex-mode count
+  SplitBuf Xin, Tb, Yk, Ub, RB, RA, RGA, RGB;
+  float *KW2 = nullptr;
+  float2 *tw = nullptr;
+  CUtensorMap mXin[2], mTb[2], mYk[2], mUb[2], mRB[2], mRA[2], mRGA[2], mRGB[2], mZmn[2];
   bool tables_ready = false;
 };
 
@@ -90,10 +98,12 @@ __device__ __forceinline__ void put_split(SplitBuf b, size_t k, double x) {
   b.lo[k] = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
 }
 
-// phi index c -> (m, is_imag)
+// phi index c -> (m, is_imag), interleaved: c = 0 -> Re m = 0, c = 1 -> Re m = Nphi/2,
+// c = 2m + ri for 1 <= m < Nphi/2 (Nphi even; the imaginary parts of m = 0 and Nphi/2 vanish)
 __device__ __forceinline__ void phi_mode(int c, int Nphi, int &m, bool &im) {
-  const int Nc = Nphi / 2 + 1;
-  if (c < Nc) { m = c; im = false; } else { m = c - Nc + 1; im = true; }
+  if (c == 0) { m = 0; im = false; }
+  else if (c == 1) { m = Nphi / 2; im = false; }
+  else { m = c >> 1; im = (c & 1) != 0; }
 }
 
 __global__ void k_tab_phi(SplitBuf F, SplitBuf Gt, int N) {
@@ -150,6 +160,43 @@ __global__ void k_tab_kw(float *KW, const double2 *khat, int Nu, int Nphi) {
     int pp = p > Nu ? p - Nu : p;
     double wgt = (p == 0 || p == Nu) ? 1.0 : 2.0;
     KW[k] = (float)(wgt / M * khat[(size_t)m * M + pp].x);
+  }
+}
+
+// Real block form [[Fr, -Fi], [Fi, Fr]] of a complex matrix F[r][k] = exp(sgn 2 pi i r k / L):
+// rows (r, ri) for r < nr, cols (k, ri') for k < nk.
+__global__ void k_tab_cblock(SplitBuf T, int nr, int nk, int L, int sgn) {
+  const size_t n = (size_t)4 * nr * nk;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int row = (int)(q / (2 * nk)), col = (int)(q % (2 * nk));
+    const int r = row >> 1, ri = row & 1, k = col >> 1, rk = col & 1;
+    double sn, cs;
+    sincospi(2.0 * (double)(((long long)r * k) % L) / L, &sn, &cs);
+    const double Fr = cs, Fi = sgn * sn;
+    const double v = (ri == 0) ? (rk == 0 ? Fr : -Fi) : (rk == 0 ? Fi : Fr);
+    put_split(T, q, v);
+  }
+}
+
+// KW2[(m, p2)][(p1, ri)] = Re khat(p2 + 64 p1, m) / M for m <= Nphi/2 (padding modes: 0)
+__global__ void k_tab_kw2(float *KW2, const double2 *khat, int nm, int A, int Nphi) {
+  const int M = 64 * A;
+  const size_t n = (size_t)nm * 64 * 2 * A;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int row = (int)(q / (2 * A)), col = (int)(q % (2 * A));
+    const int m = row >> 6, p2 = row & 63, p1 = col >> 1;
+    KW2[q] = (m <= Nphi / 2) ? (float)(khat[(size_t)m * M + p2 + 64 * p1].x / M) : 0.f;
+  }
+}
+
+// twiddles W_M^{p2 i1}, [64][A]
+__global__ void k_tab_tw(float2 *tw, int A) {
+  const int M = 64 * A;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 64 * A; q += gridDim.x * blockDim.x) {
+    const int p2 = q / A, i1 = q % A;
+    double sn, cs;
+    sincospi(2.0 * (double)(((long long)p2 * i1) % M) / M, &sn, &cs);
+    tw[q] = make_float2((float)cs, (float)-sn);
   }
 }
 
@@ -379,6 +426,50 @@ int dg_handle::mixed_init() {
              make_map(&X.mZ[0], X.Z.hi, Nu, Nphi, tc::BM) && make_map(&X.mZ[1], X.Z.lo, Nu, Nphi, tc::BM) &&
              make_map(&X.mGphi[0], X.Gphi.hi, Nphi, Nphi, tc::BN) && make_map(&X.mGphi[1], X.Gphi.lo, Nphi, Nphi, tc::BN);
   if (!okm) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed");
+  // factored u-direction when Nu is a multiple of 1024 (F1: 64-point stage on 128 rows)
+  X.factored = (Nu % 1024 == 0);
+  if (X.factored) {
+    const int A = Nu / 32, nm = ((Nphi / 2 + 1) + 3) / 4 * 4;
+    X.fa = A;
+    X.nm = nm;
+    XK(alloc_split(X.Xin, (size_t)64 * nm * A));
+    XK(cudaMemset(X.Xin.hi, 0, sizeof(__nv_bfloat16) * 64 * nm * A));
+    XK(cudaMemset(X.Xin.lo, 0, sizeof(__nv_bfloat16) * 64 * nm * A));
+    XK(alloc_split(X.Tb, (size_t)2 * A * nm * 64));
+    XK(alloc_split(X.Yk, (size_t)nm * 64 * 2 * A));
+    XK(alloc_split(X.Ub, (size_t)nm * A * 128));
+    XK(alloc_split(X.RB, (size_t)128 * 64));
+    XK(alloc_split(X.RA, (size_t)2 * A * 2 * A));
+    XK(alloc_split(X.RGA, (size_t)2 * A * 2 * A));
+    XK(alloc_split(X.RGB, (size_t)64 * 128));
+    XK(dalloc(&X.KW2, (size_t)nm * 64 * 2 * A));
+    XK(dalloc(&X.tw, (size_t)64 * A));
+    k_tab_cblock<<<64, 256, 0, st>>>(X.RB, 64, 32, 64, -1);    // W_64^{p2 i2}, i2 < 32
+    k_tab_cblock<<<64, 256, 0, st>>>(X.RA, A, A, A, -1);       // W_A^{p1 i1}
+    k_tab_cblock<<<64, 256, 0, st>>>(X.RGA, A, A, A, +1);      // W_A^{-i1 p1}
+    k_tab_cblock<<<64, 256, 0, st>>>(X.RGB, 32, 64, 64, +1);   // W_64^{-i2 p2}
+    k_tab_kw2<<<grid_for((size_t)nm * 128 * A), 256, 0, st>>>(X.KW2, Khat, nm, A, Nphi);
+    k_tab_tw<<<64, 256, 0, st>>>(X.tw, A);
+    XK(cudaGetLastError());
+    bool okf = make_map(&X.mXin[0], X.Xin.hi, 64, (uint64_t)nm * A, 64) && make_map(&X.mXin[1], X.Xin.lo, 64, (uint64_t)nm * A, 64) &&
+               make_map(&X.mTb[0], X.Tb.hi, 2 * A, (uint64_t)nm * 64, 64) && make_map(&X.mTb[1], X.Tb.lo, 2 * A, (uint64_t)nm * 64, 64) &&
+               make_map(&X.mYk[0], X.Yk.hi, (uint64_t)nm * 64, 2 * A, tc::BM) && make_map(&X.mYk[1], X.Yk.lo, (uint64_t)nm * 64, 2 * A, tc::BM) &&
+               make_map(&X.mUb[0], X.Ub.hi, (uint64_t)nm * A, 128, tc::BM) && make_map(&X.mUb[1], X.Ub.lo, (uint64_t)nm * A, 128, tc::BM) &&
+               make_map(&X.mRB[0], X.RB.hi, 128, 64, tc::BM) && make_map(&X.mRB[1], X.RB.lo, 128, 64, tc::BM) &&
+               make_map(&X.mRA[0], X.RA.hi, 2 * A, 2 * A, tc::BN) && make_map(&X.mRA[1], X.RA.lo, 2 * A, 2 * A, tc::BN) &&
+               make_map(&X.mRGA[0], X.RGA.hi, 2 * A, 2 * A, tc::BN) && make_map(&X.mRGA[1], X.RGA.lo, 2 * A, 2 * A, tc::BN) &&
+               make_map(&X.mRGB[0], X.RGB.hi, 64, 128, tc::BN) && make_map(&X.mRGB[1], X.RGB.lo, 64, 128, tc::BN) &&
+               make_map(&X.mZmn[0], X.Z.hi, Nphi, Nu, 64) && make_map(&X.mZmn[1], X.Z.lo, Nphi, Nu, 64);
+    if (!okf) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed (factored path)");
+    const void *fns[] = {(const void *)tc::k_gemm_split<tc::kEpiPhiToXin>,
+                         (const void *)tc::k_gemm_split<tc::kEpiTwiddleF1, false, true>,
+                         (const void *)tc::k_gemm_split<tc::kEpiSplitScaled, true, false>,
+                         (const void *)tc::k_gemm_split<tc::kEpiTwiddleI1>,
+                         (const void *)tc::k_gemm_split<tc::kEpiI2ToZ>,
+                         (const void *)tc::k_gemm_split<tc::kEpiRowScaleF32, true, false>};
+    for (const void *f : fns)
+      XK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kSmemBytes));
+  }
   XK(cudaFuncSetAttribute(tc::k_gemm_split<tc::kEpiSplit>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)tc::kSmemBytes));
   XK(cudaFuncSetAttribute(tc::k_gemm_split<tc::kEpiSplitScaled>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -408,9 +499,10 @@ void dg_handle::mixed_release() {
     if (X.u[b]) cudaFree(X.u[b]);
     if (X.w[b]) cudaFree(X.w[b]);
   }
-  SplitBuf *bufs[] = {&X.Sx, &X.X1, &X.Wt, &X.Z, &X.Fphi, &X.Cu, &X.CuT, &X.Gphi};
+  SplitBuf *bufs[] = {&X.Sx, &X.X1, &X.Wt, &X.Z, &X.Fphi, &X.Cu, &X.CuT, &X.Gphi,
+                      &X.Xin, &X.Tb, &X.Yk, &X.Ub, &X.RB, &X.RA, &X.RGA, &X.RGB};
   for (SplitBuf *b : bufs) free_split(*b);
-  void *ptrs[] = {X.KW, X.dPhi, X.phiscale, X.rowbuf, X.rowbufd};
+  void *ptrs[] = {X.KW, X.dPhi, X.phiscale, X.rowbuf, X.rowbufd, X.KW2, X.tw};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   delete mx;
@@ -564,13 +656,14 @@ static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *
   return cudaGetLastError();
 }
 
-template <int MODE>
+template <int MODE, bool A_MN = false, bool B_MN = false>
 static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUtensorMap &Bh, const CUtensorMap &Bl,
                         int M, int N, int K, const tc::GemmArgs &base, cudaStream_t st) {
   tc::GemmArgs a = base;
   a.M = M; a.N = N; a.K = K;
+  if (M % tc::BM || N % tc::BN || K % tc::BK) return cudaErrorInvalidValue;
   dim3 grid(N / tc::BN, M / tc::BM);
-  tc::k_gemm_split<MODE><<<grid, tc::kThreads, tc::kSmemBytes, st>>>(Ah, Al, Bh, Bl, a);
+  tc::k_gemm_split<MODE, A_MN, B_MN><<<grid, tc::kThreads, tc::kSmemBytes, st>>>(Ah, Al, Bh, Bl, a);
   return cudaGetLastError();
 }
 
@@ -580,6 +673,29 @@ int dg_handle::mixed_gravity() {
   const int Nu = p.Nu, Nphi = p.Nphi;
   tc::GemmArgs a{};
   a.status = &ctl->status;
+  if (X.factored) {
+    const int A = X.fa, nm = X.nm;
+    a.fa = A; a.nphi = Nphi; a.nmodes = nm; a.twiddle = X.tw;
+    // G1: phi DFT, stored as the F1 operand Xin[(i2, ri)][(m, i1)]
+    a.out_hi = X.Xin.hi; a.out_lo = X.Xin.lo;
+    XK(gemm<tc::kEpiPhiToXin>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st));
+    // F1: 64-point DFT over i2 (K = 32 complex), twiddle, -> Tb[(i1, ri)][(m, p2)]
+    a.out_hi = X.Tb.hi; a.out_lo = X.Tb.lo;
+    XK((gemm<tc::kEpiTwiddleF1, false, true>(X.mRB[0], X.mRB[1], X.mXin[0], X.mXin[1], 128, nm * A, 64, a, st)));
+    // F2: A-point DFT over i1, x khat / M -> Yk[(m, p2)][(p1, ri)]
+    a.out_hi = X.Yk.hi; a.out_lo = X.Yk.lo; a.ldo = 2 * A; a.table = X.KW2;
+    XK((gemm<tc::kEpiSplitScaled, true, false>(X.mTb[0], X.mTb[1], X.mRA[0], X.mRA[1], nm * 64, 2 * A, 2 * A, a, st)));
+    // I1: inverse A-point DFT over p1, conjugate twiddle -> Ub[(m, i1)][(p2, ri)]
+    a.out_hi = X.Ub.hi; a.out_lo = X.Ub.lo; a.table = nullptr;
+    XK(gemm<tc::kEpiTwiddleI1>(X.mYk[0], X.mYk[1], X.mRGA[0], X.mRGA[1], nm * 64, 2 * A, 2 * A, a, st));
+    // I2: inverse 64-point DFT over p2 (the 32 physical i2) -> Z[c][i]
+    a.out_hi = X.Z.hi; a.out_lo = X.Z.lo;
+    XK(gemm<tc::kEpiI2ToZ>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st));
+    // G4: inverse phi DFT with Z as an MN-major operand
+    a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi; a.row_scale = X.phiscale;
+    XK((gemm<tc::kEpiRowScaleF32, true, false>(X.mZmn[0], X.mZmn[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st)));
+    return DG_OK;
+  }
   // G1: X1[c][i] = Fphi[c][:] . Sx[i][:]
   a.out_hi = X.X1.hi; a.out_lo = X.X1.lo; a.ldo = Nu;
   XK(gemm<tc::kEpiSplit>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st));

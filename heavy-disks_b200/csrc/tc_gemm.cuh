@@ -35,6 +35,11 @@ enum EpiMode : int {
   kEpiSplit = 0,        // out_hi/out_lo[row][col] = split(D)
   kEpiSplitScaled = 1,  // out = split(D * table[row][col])
   kEpiRowScaleF32 = 2,  // out_f32[row][col] = D * row_scale[row]
+  // factored u-direction convolution (mixed.cu documents the index maps)
+  kEpiPhiToXin = 3,     // phi spectrum row c, column i  -> Xin[(i2, ri)][(m, i1)]
+  kEpiTwiddleF1 = 4,    // rows (p2, ri), cols (m, i1): x W_M^{p2 i1} -> T[(i1, ri)][(m, p2)]
+  kEpiTwiddleI1 = 5,    // rows (m, p2), cols (i1, ri): x W_M^{-p2 i1} -> U[(m, i1)][(p2, ri)]
+  kEpiI2ToZ = 6,        // rows (m, i1), cols (i2, ri) -> Z[c(m, ri)][i1 + A i2]
 };
 
 struct GemmArgs {
@@ -45,6 +50,9 @@ struct GemmArgs {
   const float *table;  // kEpiSplitScaled, row stride ldo
   const float *row_scale;
   int *status;         // kSt* bits raised on a bounded-wait timeout
+  // factored u-direction: A = i1 range (Nu / 32), Nphi, padded complex-mode count
+  int fa, nphi, nmodes;
+  const float2 *twiddle;  // W_M^{p2 i1}, [64][fa]
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -114,9 +122,25 @@ __device__ __forceinline__ uint64_t sdesc_sw128(const void *p) {
   return d;
 }
 
-// Instruction descriptor: kind::f16, A = B = BF16, D = F32, both K-major, M x N.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// Shared-memory matrix descriptor: MN-major, 128-byte swizzle.  The tile is stored as
+// 64-element MN chunks (lbo bytes apart) of K rows of 128 bytes, 8-row groups 1024 bytes
+// apart; one 16-deep K step is 16 rows = 2048 bytes.
+__device__ __forceinline__ uint64_t sdesc_mn_sw128(const void *p, uint32_t lbo) {
+  uint64_t a = smem_u32(p);
+  uint64_t d = 0;
+  d |= (a >> 4) & 0x3FFFull;
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;  // leading byte offset: next MN chunk
+  d |= (uint64_t)(1024 >> 4) << 32;             // stride byte offset: next 8 K rows
+  d |= 1ull << 46;
+  d |= 2ull << 61;
+  return d;
+}
+
+// Instruction descriptor: kind::f16, A = B = BF16, D = F32, M x N; a_mn / b_mn select
+// MN-major operands.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool a_mn = false, bool b_mn = false) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
@@ -151,7 +175,77 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bflo
   lo = __float2bfloat16_rn(x - __bfloat162float(hi));
 }
 
+// Epilogues of the factored u-direction passes: 32 accumulator columns starting at col of
+// one row.  Index maps (mixed.cu): i = i1 + A i2 (A = args.fa, i2 < 32), p = p2 + 64 p1,
+// complex modes m in [0, nmodes), phi index c(m, ri): c = 0 -> (0, re), c = 1 ->
+// (Nphi/2, re), c >= 2 -> (c / 2, c % 2).
 template <int MODE>
+__device__ __forceinline__ void epi_factored(const GemmArgs &a, int row, int col, const uint32_t (&r)[32], int lane) {
+  auto put = [&](size_t k, float x) {
+    __nv_bfloat16 h, l;
+    split_bf16(x, h, l);
+    a.out_hi[k] = h;
+    a.out_lo[k] = l;
+  };
+  const int A = a.fa;
+  if (MODE == kEpiPhiToXin) {
+    // rows c of the phi spectrum, columns i -> Xin[(i2, ri)][(m, i1)], ld = nmodes * A
+    const int c = row;
+    const int m = (c == 0) ? 0 : (c == 1 ? a.nphi / 2 : c >> 1);
+    const int ri = (c < 2) ? 0 : (c & 1);
+    const size_t ld = (size_t)a.nmodes * A;
+#pragma unroll 4
+    for (int q = 0; q < 32; ++q) {
+      const int i = col + q, i1 = i % A, i2 = i / A;
+      put((size_t)(i2 * 2 + ri) * ld + (size_t)m * A + i1, __uint_as_float(r[q]));
+    }
+  } else if (MODE == kEpiTwiddleF1) {
+    // rows (p2, ri) (re / im in lanes l, l^1), cols (m, i1) -> T[(i1, ri)][(m, p2)], ld = nmodes * 64
+    const int p2 = row >> 1, ri = row & 1;
+    const size_t ld = (size_t)a.nmodes * 64;
+#pragma unroll 4
+    for (int q = 0; q < 32; ++q) {
+      const float v = __uint_as_float(r[q]);
+      const float o = __shfl_xor_sync(0xffffffffu, v, 1);
+      const float re = ri ? o : v, im = ri ? v : o;
+      const int n = col + q, m = n / A, i1 = n % A;
+      const float2 w = a.twiddle[p2 * A + i1];
+      const float out = ri ? (re * w.y + im * w.x) : (re * w.x - im * w.y);
+      put((size_t)(i1 * 2 + ri) * ld + (size_t)m * 64 + p2, out);
+    }
+  } else if (MODE == kEpiTwiddleI1) {
+    // rows (m, p2), cols (i1, ri) pairs in-thread: x conj(W_M^{p2 i1}) -> U[(m, i1)][(p2, ri)], ld = 128
+    const int m = row >> 6, p2 = row & 63;
+#pragma unroll 4
+    for (int q = 0; q < 32; q += 2) {
+      const float re = __uint_as_float(r[q]), im = __uint_as_float(r[q + 1]);
+      const int i1 = (col + q) >> 1;
+      const float2 w = a.twiddle[p2 * A + i1];
+      const float ore = re * w.x + im * w.y, oim = im * w.x - re * w.y;
+      const size_t k = ((size_t)m * A + i1) * 128 + (size_t)p2 * 2;
+      put(k, ore);
+      put(k + 1, oim);
+    }
+  } else if (MODE == kEpiI2ToZ) {
+    // rows (m, i1), cols (i2, ri) -> Z[c(m, ri)][i1 + A i2] (MN-major operand of the inverse phi GEMM)
+    const int m = row / A, i1 = row % A;
+    const int half = a.nphi / 2;
+    if (m > half) return;  // padding modes
+#pragma unroll 4
+    for (int q = 0; q < 32; ++q) {
+      const int n = col + q, i2 = n >> 1, ri = n & 1;
+      int c;
+      if (m == 0) c = ri ? -1 : 0;
+      else if (m == half) c = ri ? -1 : 1;
+      else c = 2 * m + ri;
+      if (c < 0) continue;  // imaginary parts of the self-conjugate modes vanish
+      const size_t Nu = (size_t)A * 32;
+      put((size_t)c * Nu + (size_t)i1 + (size_t)A * i2, __uint_as_float(r[q]));
+    }
+  }
+}
+
+template <int MODE, bool A_MN = false, bool B_MN = false>
 __global__ void __launch_bounds__(kThreads, 1)
     k_gemm_split(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                  const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, GemmArgs args) {
@@ -192,10 +286,22 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (abort_flag) break;
       uint8_t *st = smem + s * kStageBytes;
       mbar_arrive_expect_tx(&full_bar[s], kStageBytes);
-      tma_load_2d(st, &tmAh, &full_bar[s], kc * BK, m0);
-      tma_load_2d(st + kTileA, &tmAl, &full_bar[s], kc * BK, m0);
-      tma_load_2d(st + 2 * kTileA, &tmBh, &full_bar[s], kc * BK, n0);
-      tma_load_2d(st + 2 * kTileA + kTileB, &tmBl, &full_bar[s], kc * BK, n0);
+      if (A_MN) {  // [K][M] in global: two 64-wide M chunks of 64 K rows
+        tma_load_2d(st, &tmAh, &full_bar[s], m0, kc * BK);
+        tma_load_2d(st + kTileA / 2, &tmAh, &full_bar[s], m0 + 64, kc * BK);
+        tma_load_2d(st + kTileA, &tmAl, &full_bar[s], m0, kc * BK);
+        tma_load_2d(st + kTileA + kTileA / 2, &tmAl, &full_bar[s], m0 + 64, kc * BK);
+      } else {
+        tma_load_2d(st, &tmAh, &full_bar[s], kc * BK, m0);
+        tma_load_2d(st + kTileA, &tmAl, &full_bar[s], kc * BK, m0);
+      }
+      if (B_MN) {  // [K][N] in global: one 64-wide N chunk
+        tma_load_2d(st + 2 * kTileA, &tmBh, &full_bar[s], n0, kc * BK);
+        tma_load_2d(st + 2 * kTileA + kTileB, &tmBl, &full_bar[s], n0, kc * BK);
+      } else {
+        tma_load_2d(st + 2 * kTileA, &tmBh, &full_bar[s], kc * BK, n0);
+        tma_load_2d(st + 2 * kTileA + kTileB, &tmBl, &full_bar[s], kc * BK, n0);
+      }
       ++issued;
     }
     // every issued copy must land before the CTA may exit
@@ -203,7 +309,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_wait(&full_bar[kc % STAGES], (kc / STAGES) & 1, args.status);
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer ----
-    const uint32_t idesc = idesc_bf16(BM, BN);
+    const uint32_t idesc = idesc_bf16(BM, BN, A_MN, B_MN);
     for (int kc = 0; kc < nk; ++kc) {
       const int s = kc % STAGES;
       if (!mbar_wait(&full_bar[s], (kc / STAGES) & 1, args.status)) {
@@ -212,14 +318,18 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       tc_fence_after();
       uint8_t *st = smem + s * kStageBytes;
-      const uint64_t dAh = sdesc_sw128(st), dAl = sdesc_sw128(st + kTileA);
-      const uint64_t dBh = sdesc_sw128(st + 2 * kTileA), dBl = sdesc_sw128(st + 2 * kTileA + kTileB);
+      const uint64_t dAh = A_MN ? sdesc_mn_sw128(st, kTileA / 2) : sdesc_sw128(st);
+      const uint64_t dAl = A_MN ? sdesc_mn_sw128(st + kTileA, kTileA / 2) : sdesc_sw128(st + kTileA);
+      const uint64_t dBh = B_MN ? sdesc_mn_sw128(st + 2 * kTileA, 0) : sdesc_sw128(st + 2 * kTileA);
+      const uint64_t dBl = B_MN ? sdesc_mn_sw128(st + 2 * kTileA + kTileB, 0) : sdesc_sw128(st + 2 * kTileA + kTileB);
+      // a 16-deep K step is 32 bytes along a K-major row, or 16 rows (2048 bytes) of an MN-major tile
+      const uint64_t stepA = A_MN ? (2048 >> 4) : (32 >> 4), stepB = B_MN ? (2048 >> 4) : (32 >> 4);
 #pragma unroll
       for (int kk = 0; kk < BK / 16; ++kk) {
-        const uint64_t off = (uint64_t)((kk * 32) >> 4);
-        mma_bf16(tmem_d, dAh + off, dBh + off, idesc, (kc | kk) != 0);
-        mma_bf16(tmem_d, dAh + off, dBl + off, idesc, 1u);
-        mma_bf16(tmem_d, dAl + off, dBh + off, idesc, 1u);
+        const uint64_t oa = (uint64_t)kk * stepA, ob = (uint64_t)kk * stepB;
+        mma_bf16(tmem_d, dAh + oa, dBh + ob, idesc, (kc | kk) != 0);
+        mma_bf16(tmem_d, dAh + oa, dBl + ob, idesc, 1u);
+        mma_bf16(tmem_d, dAl + oa, dBh + ob, idesc, 1u);
       }
       mma_commit(&empty_bar[s]);
     }
@@ -237,6 +347,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t r[32];
       tmem_ld32(tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
       const int col = n0 + c0;
+      if (MODE >= kEpiPhiToXin) {
+        epi_factored<MODE>(args, row, col, r, lane);
+        continue;
+      }
       if (MODE == kEpiRowScaleF32) {
         const float sc = args.row_scale[row];
         float4 *o = reinterpret_cast<float4 *>(args.out_f32 + (size_t)row * args.ldo + col);

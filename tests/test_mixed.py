@@ -25,7 +25,7 @@ def _field(Nu, Nphi, seed=0):
     return S0[:, None] * (1 + pert) + 1e-3 * rng.random((Nu, Nphi))
 
 
-@pytest.mark.parametrize("Nu,Nphi", [(128, 128), (256, 256), (128, 384), (512, 256)])
+@pytest.mark.parametrize("Nu,Nphi", [(128, 128), (256, 256), (128, 384), (512, 256), (1024, 256), (1024, 1024)])
 def test_tensor_core_potential_vs_fp64(Nu, Nphi):
     """The 4-GEMM split-BF16 DFT convolution against the FP64 FFT potential (<= 2e-4 rel)."""
     Sig = _field(Nu, Nphi)
