@@ -381,6 +381,38 @@ static void free_split(SplitBuf &b) {
   b.hi = b.lo = nullptr;
 }
 
+template <int MODE, bool A_MN = false, bool B_MN = false>
+static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUtensorMap &Bh, const CUtensorMap &Bl,
+                        int M, int N, int K, const tc::GemmArgs &base, cudaStream_t st) {
+  tc::GemmArgs a = base;
+  a.M = M; a.N = N; a.K = K;
+  if (M % tc::BM || N % tc::BN || K % tc::BK) return cudaErrorInvalidValue;
+  dim3 grid(N / tc::BN, M / tc::BM);
+  // short contractions (one or two K chunks) need no deep pipeline: fewer stages let more
+  // CTAs share an SM and hide each tile's load / epilogue latency
+  const int nk = K / tc::BK;
+  if (nk <= 1) {
+    tc::k_gemm_split<MODE, A_MN, B_MN, 1><<<grid, tc::kThreads, tc::smem_bytes(1), st>>>(Ah, Al, Bh, Bl, a);
+  } else if (nk <= 2) {
+    tc::k_gemm_split<MODE, A_MN, B_MN, 2><<<grid, tc::kThreads, tc::smem_bytes(2), st>>>(Ah, Al, Bh, Bl, a);
+  } else {
+    tc::k_gemm_split<MODE, A_MN, B_MN, tc::STAGES><<<grid, tc::kThreads, tc::smem_bytes(tc::STAGES), st>>>(Ah, Al, Bh, Bl, a);
+  }
+  return cudaGetLastError();
+}
+
+// The smem limit of every instantiation gemm() may launch, raised once at set-up.
+template <int MODE, bool A_MN, bool B_MN>
+static cudaError_t prepare_gemm() {
+  cudaError_t e;
+  e = cudaFuncSetAttribute(tc::k_gemm_split<MODE, A_MN, B_MN, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::smem_bytes(1));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(tc::k_gemm_split<MODE, A_MN, B_MN, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::smem_bytes(2));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(tc::k_gemm_split<MODE, A_MN, B_MN, tc::STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)tc::smem_bytes(tc::STAGES));
+}
+
 int dg_handle::mixed_init() {
   const int Nu = p.Nu, Nphi = p.Nphi;
   if (Nu % tc::BM || Nphi % tc::BM) {
@@ -461,21 +493,16 @@ int dg_handle::mixed_init() {
                make_map(&X.mRGB[0], X.RGB.hi, 64, 128, tc::BN) && make_map(&X.mRGB[1], X.RGB.lo, 64, 128, tc::BN) &&
                make_map(&X.mZmn[0], X.Z.hi, Nphi, Nu, 64) && make_map(&X.mZmn[1], X.Z.lo, Nphi, Nu, 64);
     if (!okf) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed (factored path)");
-    const void *fns[] = {(const void *)tc::k_gemm_split<tc::kEpiPhiToXin>,
-                         (const void *)tc::k_gemm_split<tc::kEpiTwiddleF1, false, true>,
-                         (const void *)tc::k_gemm_split<tc::kEpiSplitScaled, true, false>,
-                         (const void *)tc::k_gemm_split<tc::kEpiTwiddleI1>,
-                         (const void *)tc::k_gemm_split<tc::kEpiI2ToZ>,
-                         (const void *)tc::k_gemm_split<tc::kEpiRowScaleF32, true, false>};
-    for (const void *f : fns)
-      XK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kSmemBytes));
+    XK((prepare_gemm<tc::kEpiPhiToXin, false, false>()));
+    XK((prepare_gemm<tc::kEpiTwiddleF1, false, true>()));
+    XK((prepare_gemm<tc::kEpiSplitScaled, true, false>()));
+    XK((prepare_gemm<tc::kEpiTwiddleI1, false, false>()));
+    XK((prepare_gemm<tc::kEpiI2ToZ, false, false>()));
+    XK((prepare_gemm<tc::kEpiRowScaleF32, true, false>()));
   }
-  XK(cudaFuncSetAttribute(tc::k_gemm_split<tc::kEpiSplit>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)tc::kSmemBytes));
-  XK(cudaFuncSetAttribute(tc::k_gemm_split<tc::kEpiSplitScaled>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)tc::kSmemBytes));
-  XK(cudaFuncSetAttribute(tc::k_gemm_split<tc::kEpiRowScaleF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)tc::kSmemBytes));
+  XK((prepare_gemm<tc::kEpiSplit, false, false>()));
+  XK((prepare_gemm<tc::kEpiSplitScaled, false, false>()));
+  XK((prepare_gemm<tc::kEpiRowScaleF32, false, false>()));
   XK(cudaStreamSynchronize(st));
   X.tables_ready = true;
   return DG_OK;
@@ -656,16 +683,6 @@ static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *
   return cudaGetLastError();
 }
 
-template <int MODE, bool A_MN = false, bool B_MN = false>
-static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUtensorMap &Bh, const CUtensorMap &Bl,
-                        int M, int N, int K, const tc::GemmArgs &base, cudaStream_t st) {
-  tc::GemmArgs a = base;
-  a.M = M; a.N = N; a.K = K;
-  if (M % tc::BM || N % tc::BN || K % tc::BK) return cudaErrorInvalidValue;
-  dim3 grid(N / tc::BN, M / tc::BM);
-  tc::k_gemm_split<MODE, A_MN, B_MN><<<grid, tc::kThreads, tc::kSmemBytes, st>>>(Ah, Al, Bh, Bl, a);
-  return cudaGetLastError();
-}
 
 // dPhi = gravity of s (the split operand in X.Sx)
 int dg_handle::mixed_gravity() {

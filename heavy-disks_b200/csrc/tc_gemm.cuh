@@ -30,6 +30,9 @@ constexpr uint32_t kTileB = BN * BK * 2;
 constexpr uint32_t kStageBytes = 2 * kTileA + 2 * kTileB;
 constexpr uint32_t kTmemCols = 64;  // power of two >= 32 and >= BN
 constexpr size_t kSmemBytes = (size_t)STAGES * kStageBytes + 1024;
+// dynamic shared memory for a pipeline of ns stages (short-K GEMMs use 1-2 stages so that
+// several CTAs share an SM)
+__host__ __device__ constexpr size_t smem_bytes(int ns) { return (size_t)ns * kStageBytes + 1024; }
 
 enum EpiMode : int {
   kEpiSplit = 0,        // out_hi/out_lo[row][col] = split(D)
@@ -181,77 +184,98 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bflo
 // (Nphi/2, re), c >= 2 -> (c / 2, c % 2).
 template <int MODE>
 __device__ __forceinline__ void epi_factored(const GemmArgs &a, int row, int col, const uint32_t (&r)[32], int lane) {
+  const int A = a.fa;  // a multiple of 32, so a 32-column chunk never straddles A
   auto put = [&](size_t k, float x) {
     __nv_bfloat16 h, l;
     split_bf16(x, h, l);
     a.out_hi[k] = h;
     a.out_lo[k] = l;
   };
-  const int A = a.fa;
   if (MODE == kEpiPhiToXin) {
-    // rows c of the phi spectrum, columns i -> Xin[(i2, ri)][(m, i1)], ld = nmodes * A
+    // rows c of the phi spectrum, columns i = i1 + A i2 -> Xin[(i2, ri)][(m, i1)], ld = nmodes * A;
+    // the chunk's 32 columns are 32 consecutive i1 of one i2: one contiguous 64-byte run
     const int c = row;
     const int m = (c == 0) ? 0 : (c == 1 ? a.nphi / 2 : c >> 1);
     const int ri = (c < 2) ? 0 : (c & 1);
-    const size_t ld = (size_t)a.nmodes * A;
-#pragma unroll 4
-    for (int q = 0; q < 32; ++q) {
-      const int i = col + q, i1 = i % A, i2 = i / A;
-      put((size_t)(i2 * 2 + ri) * ld + (size_t)m * A + i1, __uint_as_float(r[q]));
+    const int i2 = col / A, i1b = col - i2 * A;
+    const size_t k0 = (size_t)(i2 * 2 + ri) * ((size_t)a.nmodes * A) + (size_t)m * A + i1b;
+    uint32_t ph[16], pl[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      __nv_bfloat16 h0, l0, h1, l1;
+      split_bf16(__uint_as_float(r[2 * q]), h0, l0);
+      split_bf16(__uint_as_float(r[2 * q + 1]), h1, l1);
+      ph[q] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+      pl[q] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+    }
+    uint4 *oh = reinterpret_cast<uint4 *>(a.out_hi + k0);
+    uint4 *ol = reinterpret_cast<uint4 *>(a.out_lo + k0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      oh[q] = make_uint4(ph[4 * q], ph[4 * q + 1], ph[4 * q + 2], ph[4 * q + 3]);
+      ol[q] = make_uint4(pl[4 * q], pl[4 * q + 1], pl[4 * q + 2], pl[4 * q + 3]);
     }
   } else if (MODE == kEpiTwiddleF1) {
     // rows (p2, ri) (re / im in lanes l, l^1), cols (m, i1) -> T[(i1, ri)][(m, p2)], ld = nmodes * 64
     const int p2 = row >> 1, ri = row & 1;
+    const int m = col / A, i1b = col - m * A;
     const size_t ld = (size_t)a.nmodes * 64;
-#pragma unroll 4
+    const size_t base = (size_t)m * 64 + p2;
+    const float2 *tw = a.twiddle + p2 * A + i1b;
+#pragma unroll
     for (int q = 0; q < 32; ++q) {
       const float v = __uint_as_float(r[q]);
       const float o = __shfl_xor_sync(0xffffffffu, v, 1);
       const float re = ri ? o : v, im = ri ? v : o;
-      const int n = col + q, m = n / A, i1 = n % A;
-      const float2 w = a.twiddle[p2 * A + i1];
+      const float2 w = __ldg(tw + q);
       const float out = ri ? (re * w.y + im * w.x) : (re * w.x - im * w.y);
-      put((size_t)(i1 * 2 + ri) * ld + (size_t)m * 64 + p2, out);
+      put((size_t)((i1b + q) * 2 + ri) * ld + base, out);
     }
   } else if (MODE == kEpiTwiddleI1) {
     // rows (m, p2), cols (i1, ri) pairs in-thread: x conj(W_M^{p2 i1}) -> U[(m, i1)][(p2, ri)], ld = 128
     const int m = row >> 6, p2 = row & 63;
-#pragma unroll 4
+    const int i1b = col >> 1;
+    const float2 *tw = a.twiddle + p2 * A + i1b;
+    const size_t base = ((size_t)m * A + i1b) * 128 + (size_t)p2 * 2;
+#pragma unroll
     for (int q = 0; q < 32; q += 2) {
       const float re = __uint_as_float(r[q]), im = __uint_as_float(r[q + 1]);
-      const int i1 = (col + q) >> 1;
-      const float2 w = a.twiddle[p2 * A + i1];
+      const float2 w = __ldg(tw + (q >> 1));
       const float ore = re * w.x + im * w.y, oim = im * w.x - re * w.y;
-      const size_t k = ((size_t)m * A + i1) * 128 + (size_t)p2 * 2;
-      put(k, ore);
-      put(k + 1, oim);
+      __nv_bfloat16 h0, l0, h1, l1;
+      split_bf16(ore, h0, l0);
+      split_bf16(oim, h1, l1);
+      const size_t k = base + (size_t)(q >> 1) * 128;
+      *reinterpret_cast<uint32_t *>(a.out_hi + k) =
+          (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+      *reinterpret_cast<uint32_t *>(a.out_lo + k) =
+          (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
     }
   } else if (MODE == kEpiI2ToZ) {
     // rows (m, i1), cols (i2, ri) -> Z[c(m, ri)][i1 + A i2] (MN-major operand of the inverse phi GEMM)
-    const int m = row / A, i1 = row % A;
+    const int m = row / A, i1 = row - m * A;
     const int half = a.nphi / 2;
     if (m > half) return;  // padding modes
-#pragma unroll 4
-    for (int q = 0; q < 32; ++q) {
-      const int n = col + q, i2 = n >> 1, ri = n & 1;
-      int c;
-      if (m == 0) c = ri ? -1 : 0;
-      else if (m == half) c = ri ? -1 : 1;
-      else c = 2 * m + ri;
-      if (c < 0) continue;  // imaginary parts of the self-conjugate modes vanish
-      const size_t Nu = (size_t)A * 32;
-      put((size_t)c * Nu + (size_t)i1 + (size_t)A * i2, __uint_as_float(r[q]));
+    const size_t Nu = (size_t)A * 32;
+    const int cre = (m == 0) ? 0 : (m == half ? 1 : 2 * m);
+    const int cim = (m == 0 || m == half) ? -1 : 2 * m + 1;  // imaginary parts of self-conjugate modes vanish
+    const int i2b = col >> 1;
+#pragma unroll
+    for (int q = 0; q < 32; q += 2) {
+      const size_t ii = (size_t)i1 + (size_t)A * (i2b + (q >> 1));
+      put((size_t)cre * Nu + ii, __uint_as_float(r[q]));
+      if (cim >= 0) put((size_t)cim * Nu + ii, __uint_as_float(r[q + 1]));
     }
   }
 }
 
-template <int MODE, bool A_MN = false, bool B_MN = false>
-__global__ void __launch_bounds__(kThreads, 1)
+template <int MODE, bool A_MN = false, bool B_MN = false, int NS = STAGES>
+__global__ void __launch_bounds__(kThreads, (NS == 1 ? 4 : (NS == 2 ? 2 : 1)))
     k_gemm_split(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                  const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, GemmArgs args) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], done_bar;
+  __shared__ __align__(8) uint64_t full_bar[NS], empty_bar[NS], done_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
 
@@ -260,7 +284,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int nk = args.K / BK;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
+    for (int s = 0; s < NS; ++s) {
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
@@ -278,8 +302,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     // ---- TMA producer ----
     int issued = 0;
     for (int kc = 0; kc < nk; ++kc) {
-      const int s = kc % STAGES;
-      if (kc >= STAGES && !mbar_wait(&empty_bar[s], ((kc / STAGES) - 1) & 1, args.status)) {
+      const int s = kc % NS;
+      if (kc >= NS && !mbar_wait(&empty_bar[s], ((kc / NS) - 1) & 1, args.status)) {
         abort_flag = 1;
         break;
       }
@@ -305,14 +329,14 @@ __global__ void __launch_bounds__(kThreads, 1)
       ++issued;
     }
     // every issued copy must land before the CTA may exit
-    for (int kc = issued > STAGES ? issued - STAGES : 0; kc < issued; ++kc)
-      mbar_wait(&full_bar[kc % STAGES], (kc / STAGES) & 1, args.status);
+    for (int kc = issued > NS ? issued - NS : 0; kc < issued; ++kc)
+      mbar_wait(&full_bar[kc % NS], (kc / NS) & 1, args.status);
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer ----
     const uint32_t idesc = idesc_bf16(BM, BN, A_MN, B_MN);
     for (int kc = 0; kc < nk; ++kc) {
-      const int s = kc % STAGES;
-      if (!mbar_wait(&full_bar[s], (kc / STAGES) & 1, args.status)) {
+      const int s = kc % NS;
+      if (!mbar_wait(&full_bar[s], (kc / NS) & 1, args.status)) {
         abort_flag = 1;
         break;
       }
