@@ -24,6 +24,7 @@
 #include "tc_gemm.cuh"
 #include "step_ctl.cuh"
 #include "hydro32w.cuh"
+#include "uconv.cuh"
 
 using namespace dg;
 
@@ -54,6 +55,10 @@ struct MixedState {
   SplitBuf Xin, Tb, Yk, Ub, RB, RA, RGA, RGB;
   float *KW2 = nullptr;
   float2 *tw = nullptr;
+  // A = 32 (Nu = 1024): the four u passes run as one fused kernel (uconv.cuh)
+  bool fused_u = false;
+  float *khm = nullptr;  // khat[m][p] / M, [nm][M]
+  float2 *twp = nullptr; // W_M^{p2 i1} with padded rows, [64][kUcTwLd]
   CUtensorMap mXin[2], mTb[2], mYk[2], mUb[2], mRB[2], mRA[2], mRGA[2], mRGB[2], mZmn[2];
   bool tables_ready = false;
 };
@@ -189,13 +194,22 @@ __global__ void k_tab_kw2(float *KW2, const double2 *khat, int nm, int A, int Np
   }
 }
 
-// twiddles W_M^{p2 i1}, [64][A]
-__global__ void k_tab_tw(float2 *tw, int A) {
+// KHM[m][p] = Re khat(p, m) / M for m <= Nphi/2 (padding modes: 0)
+__global__ void k_tab_khm(float *KHM, const double2 *khat, int nm, int M, int Nphi) {
+  const size_t n = (size_t)nm * M;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int m = (int)(q / M);
+    KHM[q] = (m <= Nphi / 2) ? (float)(khat[q].x / M) : 0.f;
+  }
+}
+
+// twiddles W_M^{p2 i1}, [64][ld] (ld >= A; columns A.. are zero)
+__global__ void k_tab_tw(float2 *tw, int A, int ld) {
   const int M = 64 * A;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 64 * A; q += gridDim.x * blockDim.x) {
-    const int p2 = q / A, i1 = q % A;
-    double sn, cs;
-    sincospi(2.0 * (double)(((long long)p2 * i1) % M) / M, &sn, &cs);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 64 * ld; q += gridDim.x * blockDim.x) {
+    const int p2 = q / ld, i1 = q % ld;
+    double sn = 0.0, cs = 0.0;
+    if (i1 < A) sincospi(2.0 * (double)(((long long)p2 * i1) % M) / M, &sn, &cs);
     tw[q] = make_float2((float)cs, (float)-sn);
   }
 }
@@ -481,8 +495,17 @@ int dg_handle::mixed_init() {
     k_tab_cblock<<<64, 256, 0, st>>>(X.RGA, A, A, A, +1);      // W_A^{-i1 p1}
     k_tab_cblock<<<64, 256, 0, st>>>(X.RGB, 32, 64, 64, +1);   // W_64^{-i2 p2}
     k_tab_kw2<<<grid_for((size_t)nm * 128 * A), 256, 0, st>>>(X.KW2, Khat, nm, A, Nphi);
-    k_tab_tw<<<64, 256, 0, st>>>(X.tw, A);
+    k_tab_tw<<<64, 256, 0, st>>>(X.tw, A, A);
     XK(cudaGetLastError());
+    X.fused_u = (A == 32);
+    if (X.fused_u) {
+      XK(dalloc(&X.khm, (size_t)nm * 64 * A));
+      XK(dalloc(&X.twp, (size_t)64 * tc::kUcTwLd));
+      k_tab_tw<<<64, 256, 0, st>>>(X.twp, A, tc::kUcTwLd);
+      k_tab_khm<<<grid_for((size_t)nm * 64 * A), 256, 0, st>>>(X.khm, Khat, nm, 64 * A, Nphi);
+      XK(cudaGetLastError());
+      XK(cudaFuncSetAttribute(tc::k_uconv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kUcSmem));
+    }
     bool okf = make_map(&X.mXin[0], X.Xin.hi, 64, (uint64_t)nm * A, 64) && make_map(&X.mXin[1], X.Xin.lo, 64, (uint64_t)nm * A, 64) &&
                make_map(&X.mTb[0], X.Tb.hi, 2 * A, (uint64_t)nm * 64, 64) && make_map(&X.mTb[1], X.Tb.lo, 2 * A, (uint64_t)nm * 64, 64) &&
                make_map(&X.mYk[0], X.Yk.hi, (uint64_t)nm * 64, 2 * A, tc::BM) && make_map(&X.mYk[1], X.Yk.lo, (uint64_t)nm * 64, 2 * A, tc::BM) &&
@@ -529,7 +552,7 @@ void dg_handle::mixed_release() {
   SplitBuf *bufs[] = {&X.Sx, &X.X1, &X.Wt, &X.Z, &X.Fphi, &X.Cu, &X.CuT, &X.Gphi,
                       &X.Xin, &X.Tb, &X.Yk, &X.Ub, &X.RB, &X.RA, &X.RGA, &X.RGB};
   for (SplitBuf *b : bufs) free_split(*b);
-  void *ptrs[] = {X.KW, X.dPhi, X.phiscale, X.rowbuf, X.rowbufd, X.KW2, X.tw};
+  void *ptrs[] = {X.KW, X.dPhi, X.phiscale, X.rowbuf, X.rowbufd, X.KW2, X.tw, X.khm, X.twp};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   delete mx;
@@ -696,18 +719,26 @@ int dg_handle::mixed_gravity() {
     // G1: phi DFT, stored as the F1 operand Xin[(i2, ri)][(m, i1)]
     a.out_hi = X.Xin.hi; a.out_lo = X.Xin.lo;
     XK(gemm<tc::kEpiPhiToXin>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st));
-    // F1: 64-point DFT over i2 (K = 32 complex), twiddle, -> Tb[(i1, ri)][(m, p2)]
-    a.out_hi = X.Tb.hi; a.out_lo = X.Tb.lo;
-    XK((gemm<tc::kEpiTwiddleF1, false, true>(X.mRB[0], X.mRB[1], X.mXin[0], X.mXin[1], 128, nm * A, 64, a, st)));
-    // F2: A-point DFT over i1, x khat / M -> Yk[(m, p2)][(p1, ri)]
-    a.out_hi = X.Yk.hi; a.out_lo = X.Yk.lo; a.ldo = 2 * A; a.table = X.KW2;
-    XK((gemm<tc::kEpiSplitScaled, true, false>(X.mTb[0], X.mTb[1], X.mRA[0], X.mRA[1], nm * 64, 2 * A, 2 * A, a, st)));
-    // I1: inverse A-point DFT over p1, conjugate twiddle -> Ub[(m, i1)][(p2, ri)]
-    a.out_hi = X.Ub.hi; a.out_lo = X.Ub.lo; a.table = nullptr;
-    XK(gemm<tc::kEpiTwiddleI1>(X.mYk[0], X.mYk[1], X.mRGA[0], X.mRGA[1], nm * 64, 2 * A, 2 * A, a, st));
-    // I2: inverse 64-point DFT over p2 (the 32 physical i2) -> Z[c][i]
-    a.out_hi = X.Z.hi; a.out_lo = X.Z.lo;
-    XK(gemm<tc::kEpiI2ToZ>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st));
+    if (X.fused_u) {
+      // F1, F2, I1, I2 in one kernel: four modes per CTA, operands kept on chip
+      tc::UconvArgs u{X.twp, X.khm, X.Z.hi, X.Z.lo, Nu, Nphi, &ctl->status};
+      tc::k_uconv<<<nm / tc::kUcModes, tc::kUcThreads, tc::kUcSmem, st>>>(
+          X.mRB[0], X.mRB[1], X.mXin[0], X.mXin[1], X.mRA[0], X.mRA[1], X.mRGA[0], X.mRGA[1], X.mRGB[0], X.mRGB[1], u);
+      XK(cudaGetLastError());
+    } else {
+      // F1: 64-point DFT over i2 (K = 32 complex), twiddle, -> Tb[(i1, ri)][(m, p2)]
+      a.out_hi = X.Tb.hi; a.out_lo = X.Tb.lo;
+      XK((gemm<tc::kEpiTwiddleF1, false, true>(X.mRB[0], X.mRB[1], X.mXin[0], X.mXin[1], 128, nm * A, 64, a, st)));
+      // F2: A-point DFT over i1, x khat / M -> Yk[(m, p2)][(p1, ri)]
+      a.out_hi = X.Yk.hi; a.out_lo = X.Yk.lo; a.ldo = 2 * A; a.table = X.KW2;
+      XK((gemm<tc::kEpiSplitScaled, true, false>(X.mTb[0], X.mTb[1], X.mRA[0], X.mRA[1], nm * 64, 2 * A, 2 * A, a, st)));
+      // I1: inverse A-point DFT over p1, conjugate twiddle -> Ub[(m, i1)][(p2, ri)]
+      a.out_hi = X.Ub.hi; a.out_lo = X.Ub.lo; a.table = nullptr;
+      XK(gemm<tc::kEpiTwiddleI1>(X.mYk[0], X.mYk[1], X.mRGA[0], X.mRGA[1], nm * 64, 2 * A, 2 * A, a, st));
+      // I2: inverse 64-point DFT over p2 (the 32 physical i2) -> Z[c][i]
+      a.out_hi = X.Z.hi; a.out_lo = X.Z.lo;
+      XK(gemm<tc::kEpiI2ToZ>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st));
+    }
     // G4: inverse phi DFT with Z as an MN-major operand
     a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi; a.row_scale = X.phiscale;
     XK((gemm<tc::kEpiRowScaleF32, true, false>(X.mZmn[0], X.mZmn[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st)));
