@@ -6,7 +6,12 @@ rank advances its own disk (independent disks, weak scaling) and `value` is the 
 zone-updates/s of the job, timed on the device as the max over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
-                  [--size 1024] [--impl ours|reference]
+                  [--size 1024] [--chunk 64] [--cold-steps 200] [--impl ours|reference]
+
+The K timed steps run as dg_run_steps calls of --chunk steps (each one launch of the
+captured step loop, the way dg_advance runs a disk), with L2 flushed before every call and
+CUDA events around it.  Then --cold-steps single steps, each after an L2 flush, give the
+cold per-step time and, with per-kernel events, the roofline of every kernel of the step.
 
 --impl reference times the reference's own CPU implementation (diskfft/src hydro.hpp +
 kalnajs.hpp compiled unmodified against the FFTW-API shim, oracle/_ref/refbench) on the
@@ -34,13 +39,16 @@ REFBENCH = os.path.join(ROOT, "oracle", "_ref", "refbench")
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10000)
+    ap.add_argument("--steps", type=int, default=10240)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--size", type=int, default=1024)
     ap.add_argument("--eps", type=float, default=0.005)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--chunk", type=int, default=64, help="steps per timed iteration (one graph launch)")
+    ap.add_argument("--cold-steps", type=int, default=200,
+                    help="single steps with a flushed L2, timed and profiled per kernel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -179,14 +187,54 @@ def physical_gpu_index(local):
 
 
 def measured_peaks():
-    """(HBM GB/s, sustained dense BF16 TFLOP/s, kind).  The sustained tensor figure applies:
-    the gravity GEMMs are timed inside a seconds-long loop of steps."""
+    """(HBM GB/s, dense BF16 TFLOP/s, kind).  The sustained tensor figure applies: the
+    gravity GEMMs are timed inside a seconds-long loop of steps."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             pk = json.load(f)
         return float(pk["hbm_gbs"]), float(pk.get("bf16_tflops_sustained", pk["bf16_tflops"])), "measured"
     except (OSError, KeyError, ValueError):
         return 6650.0, 1400.0, "fallback"
+
+
+def ncu_traffic(precision, size):
+    """DRAM bytes per launch of each kernel (dram__bytes_read.sum + dram__bytes_write.sum)
+    from the committed ncu summary of this workload, or {} when none was captured."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            return json.load(f).get(f"{precision}_{size}", {})
+    except (OSError, ValueError):
+        return {}
+
+
+def gravity_parts(precision, Nu, Nphi):
+    """(phase, kernel, bound, work per launch, unit of work) of the three gravity parts."""
+    M = 2 * Nu
+    if precision == "fp64":
+        # HBM-bound FFT passes; algorithmic bytes: Sigma in + half spectrum out (phi forward),
+        # spectrum in/out + khat (u convolution), spectrum in + Phi out (phi inverse)
+        nc = Nphi // 2 + 1
+        spec = 16 * M * nc
+        return [("grav_phi_fwd", "FP64 smem FFT, phi forward (k_phi_fwd)", "hbm", 8 * Nu * Nphi + spec, "B"),
+                ("grav_u", "FP64 smem FFT, u convolution x khat (k_u_conv)", "hbm", 2 * spec + spec, "B"),
+                ("grav_phi_inv", "FP64 smem FFT, phi inverse + scaling (k_phi_inv)", "hbm", spec + 8 * Nu * Nphi, "B")]
+    # split-BF16 tcgen05 products: 3 MMAs per term, 2 flops per MAC
+    g1 = 6 * Nphi * Nu * Nphi
+    g4 = 6 * Nu * Nphi * Nphi
+    if Nu % 1024 == 0:
+        A, nm = Nu // 32, ((Nphi // 2 + 1) + 3) // 4 * 4
+        u = 6 * 128 * (nm * A) * 64 + 2 * 6 * (nm * 64) * (2 * A) * (2 * A) + 6 * (nm * A) * 64 * 128
+        uname = ("fused factored u convolution (k_uconv: 64 x 32 Cooley-Tukey in four tcgen05 stages)"
+                 if Nu == 1024 else "factored u convolution (four k_gemm_split passes)")
+    else:
+        u = 6 * Nphi * 2 * Nu * Nu + 6 * Nu * Nphi * 2 * Nu
+        uname = "dense u DFT x khat (two k_gemm_split passes)"
+    return [("grav_phi_fwd", "phi DFT GEMM (k_gemm_split, split-BF16)", "tensor", g1, "flop"),
+            ("grav_u", uname, "tensor", u, "flop"),
+            ("grav_phi_inv", "inverse phi DFT GEMM + potential scaling (k_gemm_split)", "tensor", g4, "flop")]
+
+
+TRAFFIC_KEYS = {"hydro": "hydro", "grav_phi_fwd": "grav_phi_fwd", "grav_u": "grav_u", "grav_phi_inv": "grav_phi_inv"}
 
 
 # ---------------------------------------------------------------------------------
@@ -219,25 +267,30 @@ def main():
     stream = torch.cuda.Stream()
     disk.set_stream(stream.cuda_stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    kps = disk.kernels_per_step()
+
+    # timed iterations: one dg_run_steps call of `chunk` steps each (a CUDA graph of the
+    # device-resident step loop, as dg_advance runs it), L2 flushed before every iteration
+    chunk = max(1, min(a.chunk, a.steps))
+    sizes = [chunk] * (a.steps // chunk) + ([a.steps % chunk] if a.steps % chunk else [])
+    warm_iters = max(3, -(-a.warmup // chunk))
 
     clk = ClockSampler(physical_gpu_index(local)).__enter__()
     with torch.cuda.stream(stream):
-        for _ in range(max(a.warmup, 3)):
+        for _ in range(warm_iters):
             flush.zero_()
-            disk.run_steps(1, 0.3, sync=False)
+            disk.run_steps(chunk, 0.3, sync=False)
         torch.cuda.synchronize()
 
-        # ---- timed region: K steps, L2 flushed (untimed) before each ----
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
-        disk.profile(True)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in sizes]
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
         t_wall0 = time.time()
-        for k in range(a.steps):
+        for k, n in enumerate(sizes):
             flush.zero_()
             ev[k][0].record(stream)
-            disk.run_steps(1, 0.3, sync=False)
+            disk.run_steps(n, 0.3, sync=False)
             ev[k][1].record(stream)
         torch.cuda.synchronize()
         clk.window = (t_wall0, time.time())
@@ -245,8 +298,6 @@ def main():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        prof = disk.profile_read()
-        disk.profile(False)
         ms = sum(s.elapsed_time(e) for s, e in ev)
     t_dev = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -256,46 +307,60 @@ def main():
     zones = N * N
     value = world * zones * a.steps / (ms_max * 1e-3)
 
-    # ---- roofline of the fused hydro kernel (HBM bound) and the gravity ----
+    # ---- single steps with a cold L2 (flushed before each), then the per-kernel split ----
+    cold_n = max(1, min(a.cold_steps, a.steps))
+    with torch.cuda.stream(stream):
+        evc = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(cold_n)]
+        for k in range(cold_n):
+            flush.zero_()
+            evc[k][0].record(stream)
+            disk.run_steps(1, 0.3, sync=False)
+            evc[k][1].record(stream)
+        torch.cuda.synchronize()
+        cold_ms = sum(s.elapsed_time(e) for s, e in evc) / cold_n
+        disk.profile(True)
+        for k in range(cold_n):
+            flush.zero_()
+            disk.run_steps(1, 0.3, sync=False)
+        torch.cuda.synchronize()
+        prof = disk.profile_read()
+        disk.profile(False)
+
+    # ---- roofline of every kernel of the step (live CUDA-event times, cold L2) ----
     hbm_peak, tc_peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic(a.precision, N)
     word = 8 if a.precision == "fp64" else 4
-    hyd_ms, hyd_n = prof["hydro"]
-    grav_ms, grav_n = prof["gravity"]
-    hyd_bytes = 7 * word * zones  # read Sigma, vR, vphi, Phi; write Sigma, vR, vphi
-    hyd_gbs = hyd_bytes / (hyd_ms / max(hyd_n, 1) * 1e-3) / 1e9 if hyd_n else None
-    roof_hydro = {"kernel": "fused hydro sweep", "bound": "hbm", "achieved": hyd_gbs, "peak": hbm_peak,
-                  "unit": "GB/s", "frac": (hyd_gbs / hbm_peak) if hyd_gbs else None, "traffic": None,
-                  "bytes_alg_per_launch": hyd_bytes, "ms_per_launch": hyd_ms / max(hyd_n, 1),
-                  "peak_kind": peak_kind}
-    share = {"hydro": hyd_ms / ms if ms else None, "gravity": grav_ms / ms if ms else None}
-    roof = roof_hydro
-    if a.precision == "fp64" and grav_n:
-        # plain path: the FFT passes are HBM bound; algorithmic bytes per launch =
-        # Sigma in (8 B/zone) + phi spectrum out/in/out/in (4 x 8 B/zone) + khat (16 B/zone) + Phi out (8)
-        g_bytes = (8 + 4 * 8 + 16 + 8) * zones
-        g_gbs = g_bytes / (grav_ms / grav_n * 1e-3) / 1e9
-        roof_grav = {"kernel": "FP64 FFT gravity (3 passes)", "bound": "hbm", "achieved": g_gbs, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": g_gbs / hbm_peak, "traffic": None, "bytes_alg_per_launch": g_bytes,
-                     "ms_per_launch": grav_ms / grav_n, "peak_kind": peak_kind}
-        if grav_ms > hyd_ms:
-            roof = roof_grav
-        roof_all = [roof_hydro, roof_grav]
-    elif grav_n:
-        # mixed path: four dense split-BF16 GEMMs, 3 tensor-core products per term
-        Nu = Nphi = N
-        alg = 4 * Nu * Nphi * Nphi + 8 * Nu * Nu * Nphi
-        g_tf = 3 * alg / (grav_ms / grav_n * 1e-3) / 1e12
-        roof_grav = {"kernel": "split-BF16 tcgen05 DFT gravity (4 GEMMs)", "bound": "tensor", "achieved": g_tf,
-                     "peak": tc_peak, "unit": "TFLOP/s", "frac": g_tf / tc_peak, "traffic": None,
-                     "flops_executed_per_launch": 3 * alg, "flops_dense_dft": alg,
-                     "ms_per_launch": grav_ms / grav_n, "peak_kind": peak_kind + " (sustained bf16)"}
-        if grav_ms > hyd_ms:
-            roof = roof_grav
-        roof_all = [roof_hydro, roof_grav]
-    else:
-        roof_all = [roof_hydro]
-    # kernels of ours per step: fp64 = 3 FFT passes + hydro; mixed = 4 GEMMs + hydro
-    launches_per_step = 4 if a.precision == "fp64" else 5
+    # read Sigma, vR, vphi, Phi; write Sigma, vR, vphi (+ the split-BF16 gravity operand,
+    # 2 x 2 bytes, that the mixed hydro kernel writes for the next step's gravity)
+    hyd_bytes = (7 * word + (4 if a.precision == "mixed" else 0)) * zones
+
+    def entry(phase, kernel, bound, work, unit_kind):
+        t, n = prof.get(phase, (0.0, 0))
+        if not n:
+            return None
+        ms1 = t / n
+        if unit_kind == "B":
+            ach, peak, unit = work / (ms1 * 1e-3) / 1e9, hbm_peak, "GB/s"
+        else:
+            ach, peak, unit = work / (ms1 * 1e-3) / 1e12, tc_peak, "TFLOP/s"
+        tr = traffic.get(TRAFFIC_KEYS.get(phase, ""))
+        e = {"kernel": kernel, "bound": bound, "achieved": ach, "peak": peak, "unit": unit, "frac": ach / peak,
+             "traffic": tr, "ms_per_launch": ms1, "share_of_step": ms1 / cold_ms,
+             "peak_kind": peak_kind + (" (sustained bf16)" if unit_kind == "flop" else " (copy)")}
+        e["bytes_alg_per_launch" if unit_kind == "B" else "flops_executed_per_launch"] = work
+        return e
+
+    hyd_name = "fused hydro sweep (k_hydro32w: source + R sweep + phi sweep + CFL)" if a.precision == "mixed" \
+        else "fused hydro sweep (k_hydro64: source + R sweep + phi sweep + CFL)"
+    roof_all = [entry("hydro", hyd_name, "hbm", hyd_bytes, "B")]
+    for ph, kern, bound, work, kind in gravity_parts(a.precision, N, N):
+        e = entry(ph, kern, bound, work, kind)
+        if e is not None and a.precision == "mixed":
+            e["flops_fft_nominal_whole_gravity"] = 5 * (2 * N * N) * int(np.log2(2 * N * N)) * 2
+        roof_all.append(e)
+    roof_all = [e for e in roof_all if e is not None]
+    roof = max(roof_all, key=lambda e: e["ms_per_launch"])
+    share = {k: v[0] / (cold_ms * cold_n) for k, v in prof.items() if v[1]}
 
     # ---- end to end through the C ABI on host buffers (pinned), every step ----
     e2e = None
@@ -325,17 +390,24 @@ def main():
 
     if rank == 0:
         cfg = workload(a)
-        cfg.update({"precision": a.precision, "l2": "flushed before every timed step (256 MiB device write, "
-                    "outside the timed events)", "stream": "caller stream via dg_set_stream",
-                    "phase_share": share})
+        cfg.update({"precision": a.precision,
+                    "timed_iteration": f"one dg_run_steps call of {chunk} steps (a CUDA graph of the "
+                                       "device-resident step loop)",
+                    "l2": f"flushed (256 MiB device write, outside the timed events) before every timed "
+                          f"iteration of {chunk} steps; within an iteration the disk's fields stay resident "
+                          "as in a production run",
+                    "cold_l2_single_step": {"ms_per_step": cold_ms, "steps": cold_n,
+                                            "note": "one step per timed iteration, L2 flushed before each"},
+                    "stream": "caller stream via dg_set_stream", "phase_share_cold": share,
+                    "kernels_per_step": kps})
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-            "warmup": max(a.warmup, 3), "ms_per_step": ms_max / a.steps, "higher_is_better": True,
+            "warmup": warm_iters * chunk, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if a.precision == "fp64" else "f32 state + f64 basic state, split-bf16 DFT",
             "data": "synthetic (standard heavy disk, seeded m=2 phase)", "config": cfg,
             "roofline": roof, "roofline_all": roof_all, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": launches_per_step * a.steps, "clocks": clk.summary(),
+            "gpu_launches": kps * a.steps, "clocks": clk.summary(),
         }
         print(json.dumps(line))
     disk.close()

@@ -190,10 +190,16 @@ void dg_handle::release() {
 // ---------------------------------------------------------------------------------
 // gravity (FP64): kalnajs.hpp:48-63
 int dg_handle::potential64(const double *dSig, double *dOut) {
+  MK(prof_begin(DG_PROF_GRAV_PHI_FWD));
   MK(launch_phi_fwd<double>(dSig, p.Nu, p.Nphi, dR32, W, M, plPhi, rootsPhi, st));
+  MK(prof_end(DG_PROF_GRAV_PHI_FWD));
+  MK(prof_begin(DG_PROF_GRAV_U));
   MK(launch_u_conv<double>(W, M, Nc, p.Nu, p.Nu, plM, rootsM, Khat, nullptr, st));
+  MK(prof_end(DG_PROF_GRAV_U));
   const double pref = -p.G * du * dphi / (static_cast<double>(M) * p.Nphi);
+  MK(prof_begin(DG_PROF_GRAV_PHI_INV));
   MK(launch_phi_inv<double>(W, M, p.Nu, p.Nphi, plPhi, rootsPhi, pref, dSqrtR, dOut, st));
+  MK(prof_end(DG_PROF_GRAV_PHI_INV));
   return DG_OK;
 }
 
@@ -236,9 +242,11 @@ cudaError_t dg_handle::prof_begin(int phase) {
 }
 
 cudaError_t dg_handle::prof_end(int phase) {
-  (void)phase;
   if (!prof_on) return cudaSuccess;
-  return cudaEventRecord(ev_pool[prof_pending.back().second + 1], st);
+  // phases nest (the gravity parts sit inside the gravity phase): close the latest of this phase
+  for (auto it = prof_pending.rbegin(); it != prof_pending.rend(); ++it)
+    if (it->first == phase) return cudaEventRecord(ev_pool[it->second + 1], st);
+  return cudaErrorInvalidValue;
 }
 
 int dg_handle::prof_collect() {
@@ -777,6 +785,12 @@ int dg_profile_enable(dg_handle *h, int on) {
   if (rc) return rc;
   h->prof_on = on != 0;
   return DG_OK;
+}
+
+int dg_kernels_per_step(const dg_handle *h) {
+  if (!h) return DG_ERR_INVALID;
+  const int grav = !h->p.selfgrav ? 0 : (h->p.precision == DG_PREC_MIXED ? h->mixed_gravity_kernels() : 3);
+  return grav + 1;
 }
 
 int dg_profile_read(dg_handle *h, double *ms, long long *count) {

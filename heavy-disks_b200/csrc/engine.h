@@ -59,8 +59,8 @@ struct dg_handle {
   std::vector<cudaEvent_t> ev_pool;
   int ev_used = 0;
   std::vector<std::pair<int, int>> prof_pending;
-  double prof_ms[DG_PROF_N] = {0, 0, 0};
-  long long prof_count[DG_PROF_N] = {0, 0, 0};
+  double prof_ms[DG_PROF_N] = {};
+  long long prof_count[DG_PROF_N] = {};
   cudaError_t prof_begin(int phase);
   cudaError_t prof_end(int phase);
   int prof_collect();
@@ -94,6 +94,7 @@ struct dg_handle {
   int mixed_upload_state(const double *Sig, const double *vR, const double *vp);
   int mixed_download_state(double *Sig, double *vR, double *vp);
   int mixed_gravity();
+  int mixed_gravity_kernels() const;
   int mixed_potential(const double *dSig, double *dOut);
   bool in_step_host = false;  // upload from dg_step_host keeps the mixed basic state
   void mixed_basic(std::vector<double> *S0, std::vector<double> *V0, std::vector<double> *g0) const;

@@ -79,6 +79,11 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // K-major BF16 matrix [rows][cols] -> tiles of box_rows x 64 with 128-byte swizzle.
+// radial-direction layout of the split-BF16 gravity: factored (M = 2 Nu = 64 x Nu/32) when
+// Nu is a multiple of 1024, and the four factored passes fused into one kernel at Nu = 1024
+static bool u_factored(int Nu) { return Nu % 1024 == 0; }
+static bool u_fused(int Nu) { return Nu == 1024; }
+
 static bool make_map(CUtensorMap *m, const void *base, uint64_t rows, uint64_t cols, uint32_t box_rows) {
   auto fn = encode_fn();
   if (!fn) return false;
@@ -473,7 +478,7 @@ int dg_handle::mixed_init() {
              make_map(&X.mGphi[0], X.Gphi.hi, Nphi, Nphi, tc::BN) && make_map(&X.mGphi[1], X.Gphi.lo, Nphi, Nphi, tc::BN);
   if (!okm) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed");
   // factored u-direction when Nu is a multiple of 1024 (F1: 64-point stage on 128 rows)
-  X.factored = (Nu % 1024 == 0);
+  X.factored = u_factored(Nu);
   if (X.factored) {
     const int A = Nu / 32, nm = ((Nphi / 2 + 1) + 3) / 4 * 4;
     X.fa = A;
@@ -497,7 +502,7 @@ int dg_handle::mixed_init() {
     k_tab_kw2<<<grid_for((size_t)nm * 128 * A), 256, 0, st>>>(X.KW2, Khat, nm, A, Nphi);
     k_tab_tw<<<64, 256, 0, st>>>(X.tw, A, A);
     XK(cudaGetLastError());
-    X.fused_u = (A == 32);
+    X.fused_u = u_fused(Nu);
     if (X.fused_u) {
       XK(dalloc(&X.khm, (size_t)nm * 64 * A));
       XK(dalloc(&X.twp, (size_t)64 * tc::kUcTwLd));
@@ -718,7 +723,10 @@ int dg_handle::mixed_gravity() {
     a.fa = A; a.nphi = Nphi; a.nmodes = nm; a.twiddle = X.tw;
     // G1: phi DFT, stored as the F1 operand Xin[(i2, ri)][(m, i1)]
     a.out_hi = X.Xin.hi; a.out_lo = X.Xin.lo;
+    XK(prof_begin(DG_PROF_GRAV_PHI_FWD));
     XK(gemm<tc::kEpiPhiToXin>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st));
+    XK(prof_end(DG_PROF_GRAV_PHI_FWD));
+    XK(prof_begin(DG_PROF_GRAV_U));
     if (X.fused_u) {
       // F1, F2, I1, I2 in one kernel: four modes per CTA, operands kept on chip
       tc::UconvArgs u{X.twp, X.khm, X.Z.hi, X.Z.lo, Nu, Nphi, &ctl->status};
@@ -739,24 +747,38 @@ int dg_handle::mixed_gravity() {
       a.out_hi = X.Z.hi; a.out_lo = X.Z.lo;
       XK(gemm<tc::kEpiI2ToZ>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st));
     }
+    XK(prof_end(DG_PROF_GRAV_U));
     // G4: inverse phi DFT with Z as an MN-major operand
     a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi; a.row_scale = X.phiscale;
+    XK(prof_begin(DG_PROF_GRAV_PHI_INV));
     XK((gemm<tc::kEpiRowScaleF32, true, false>(X.mZmn[0], X.mZmn[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st)));
+    XK(prof_end(DG_PROF_GRAV_PHI_INV));
     return DG_OK;
   }
   // G1: X1[c][i] = Fphi[c][:] . Sx[i][:]
   a.out_hi = X.X1.hi; a.out_lo = X.X1.lo; a.ldo = Nu;
+  XK(prof_begin(DG_PROF_GRAV_PHI_FWD));
   XK(gemm<tc::kEpiSplit>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st));
+  XK(prof_end(DG_PROF_GRAV_PHI_FWD));
   // G2: Wt[c][p] = KW[c][p] * X1[c][:] . Cu[p][:]
   a.out_hi = X.Wt.hi; a.out_lo = X.Wt.lo; a.ldo = 2 * Nu; a.table = X.KW;
+  XK(prof_begin(DG_PROF_GRAV_U));
   XK(gemm<tc::kEpiSplitScaled>(X.mX1[0], X.mX1[1], X.mCu[0], X.mCu[1], Nphi, 2 * Nu, Nu, a, st));
   // G3: Z[i][c] = CuT[i][:] . Wt[c][:]
   a.out_hi = X.Z.hi; a.out_lo = X.Z.lo; a.ldo = Nphi; a.table = nullptr;
   XK(gemm<tc::kEpiSplit>(X.mCuT[0], X.mCuT[1], X.mWt[0], X.mWt[1], Nu, Nphi, 2 * Nu, a, st));
+  XK(prof_end(DG_PROF_GRAV_U));
   // G4: dPhi[i][j] = phiscale[i] * Z[i][:] . Gphi[j][:]
   a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi; a.row_scale = X.phiscale;
+  XK(prof_begin(DG_PROF_GRAV_PHI_INV));
   XK(gemm<tc::kEpiRowScaleF32>(X.mZ[0], X.mZ[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st));
+  XK(prof_end(DG_PROF_GRAV_PHI_INV));
   return DG_OK;
+}
+
+int dg_handle::mixed_gravity_kernels() const {
+  if (!u_factored(p.Nu)) return 4;
+  return u_fused(p.Nu) ? 3 : 6;
 }
 
 int dg_handle::mixed_enqueue_step() {

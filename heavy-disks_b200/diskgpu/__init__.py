@@ -57,7 +57,7 @@ EXPORTS = (
     "dg_params_default", "dg_create", "dg_destroy", "dg_last_error", "dg_status_string", "dg_grid",
     "dg_init_standard", "dg_set_state", "dg_get_state", "dg_timestep", "dg_step", "dg_step_forces",
     "dg_potential", "dg_forces", "dg_disk_mass", "dg_modes", "dg_conserved", "dg_advance", "dg_time",
-    "dg_set_stream", "dg_run_steps", "dg_step_host", "dg_profile_enable", "dg_profile_read",
+    "dg_set_stream", "dg_run_steps", "dg_step_host", "dg_profile_enable", "dg_profile_read", "dg_kernels_per_step",
     "dg_timestep_static", "dg_rotation_curve_elliptic", "dg_params_physical",
     "dg_batch_create", "dg_batch_destroy", "dg_batch_last_error", "dg_batch_size", "dg_batch_disk",
     "dg_batch_init_standard", "dg_batch_advance", "dg_save", "dg_load", "dg_set_diagnostics",
@@ -67,7 +67,8 @@ EXPORTS = (
 
 BASIC_FFT, BASIC_ELLIPTIC = 0, 1
 
-PROF_HYDRO, PROF_GRAVITY, PROF_CFL, PROF_N = 0, 1, 2, 3
+PROF_HYDRO, PROF_GRAVITY, PROF_CFL, PROF_GRAV_PHI_FWD, PROF_GRAV_U, PROF_GRAV_PHI_INV, PROF_N = 0, 1, 2, 3, 4, 5, 6
+PROF_NAMES = ("hydro", "gravity", "cfl", "grav_phi_fwd", "grav_u", "grav_phi_inv")
 
 _lib = None
 
@@ -111,6 +112,7 @@ def lib():
     L.dg_step_host.argtypes = [H, C.c_double, D, D, D, D]
     L.dg_profile_enable.argtypes = [H, C.c_int]
     L.dg_profile_read.argtypes = [H, D, C.POINTER(C.c_longlong)]
+    L.dg_kernels_per_step.argtypes = [H]
     L.dg_rotation_curve_elliptic.argtypes = [C.POINTER(Params), C.c_int, D, D, D, D, D]
     L.dg_params_physical.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(Params), D]
     L.dg_batch_create.argtypes = [C.c_int, C.POINTER(Params), C.POINTER(H)]
@@ -366,8 +368,14 @@ class Disk:
         ms = np.zeros(PROF_N)
         cnt = (C.c_longlong * PROF_N)()
         self._ck(lib().dg_profile_read(self.h, _dp(ms), cnt))
-        names = ("hydro", "gravity", "cfl")
-        return {names[k]: (float(ms[k]), int(cnt[k])) for k in range(PROF_N)}
+        return {PROF_NAMES[k]: (float(ms[k]), int(cnt[k])) for k in range(PROF_N)}
+
+    def kernels_per_step(self):
+        """How many of this library's kernels one time step launches."""
+        n = lib().dg_kernels_per_step(self.h)
+        if n < 0:
+            raise DiskGPUError(n, "dg_kernels_per_step")
+        return n
 
 
 class _BorrowedDisk(Disk):

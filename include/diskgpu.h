@@ -222,13 +222,19 @@ int dg_run_steps(dg_handle *h, int nsteps, double cfl, int sync);
 int dg_step_host(dg_handle *h, double cfl, double *Sig, double *vR, double *vp, double *dt);
 
 /* Per-phase device timing with CUDA events on the handle's stream. */
-#define DG_PROF_HYDRO 0   /* fused hydro kernel */
-#define DG_PROF_GRAVITY 1 /* whole gravity convolution */
-#define DG_PROF_CFL 2     /* standalone CFL reductions */
-#define DG_PROF_N 3
+#define DG_PROF_HYDRO 0         /* fused hydro kernel */
+#define DG_PROF_GRAVITY 1       /* whole gravity convolution */
+#define DG_PROF_CFL 2           /* standalone CFL reductions */
+#define DG_PROF_GRAV_PHI_FWD 3  /* gravity, part: forward phi transform (FP64 FFT pass / phi DFT GEMM) */
+#define DG_PROF_GRAV_U 4        /* gravity, part: radial convolution with khat */
+#define DG_PROF_GRAV_PHI_INV 5  /* gravity, part: inverse phi transform and potential scaling */
+#define DG_PROF_N 6
 int dg_profile_enable(dg_handle *h, int on);
 /* Accumulated milliseconds and launch counts per phase since the last read (resets). */
 int dg_profile_read(dg_handle *h, double *ms, long long *count);
+/* Number of this library's kernels one time step of the handle launches (gravity passes
+ * plus the fused hydro kernel); depends on precision, grid and self-gravity. */
+int dg_kernels_per_step(const dg_handle *h);
 
 /* Allocation-free CFL time step.  No counterpart in the reference: it is the same
  * dt = cfl / max_ij (sR + sphi) as dg_timestep, for callers that may not allocate device
