@@ -350,8 +350,8 @@ def main():
         e["bytes_alg_per_launch" if unit_kind == "B" else "flops_executed_per_launch"] = work
         return e
 
-    hyd_name = "fused hydro sweep (k_hydro32w: source + R sweep + phi sweep + CFL)" if a.precision == "mixed" \
-        else "fused hydro sweep (k_hydro64: source + R sweep + phi sweep + CFL)"
+    hyd_name = "fused hydro sweep (k_hydro32t: 16 x 58 tiles, source + R sweep + phi sweep + CFL)" \
+        if a.precision == "mixed" else "fused hydro sweep (k_hydro64: source + R sweep + phi sweep + CFL)"
     roof_all = [entry("hydro", hyd_name, "hbm", hyd_bytes, "B")]
     for ph, kern, bound, work, kind in gravity_parts(a.precision, N, N):
         e = entry(ph, kern, bound, work, kind)

@@ -57,6 +57,14 @@ __device__ __forceinline__ V cmul(V a, V b) {
   return r;
 }
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream serialization
+// may start while the kernel before it on the stream is still running: it does its
+// prologue (shared memory, TMEM, constant tables), then pdl_wait() blocks until that kernel
+// (and, transitively, everything before it) has completed with its writes visible.  With no
+// such predecessor pdl_wait() returns at once.  pdl_trigger() lets the next kernel start.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Ordered atomic max for non-negative doubles (NaN compares above +inf, so a NaN
 // propagates into the max and is caught by the non-finite check).
 __device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double v) {

@@ -14,7 +14,9 @@
 // Each GEMM's epilogue writes the next GEMM's operand as a BF16 (hi, lo) pair in the
 // K-major layout it needs; the hydro kernel writes s for G1 and reads dPhi.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -24,6 +26,7 @@
 #include "tc_gemm.cuh"
 #include "step_ctl.cuh"
 #include "hydro32w.cuh"
+#include "hydro32t.cuh"
 #include "uconv.cuh"
 
 using namespace dg;
@@ -55,6 +58,9 @@ struct MixedState {
   SplitBuf Xin, Tb, Yk, Ub, RB, RA, RGA, RGB;
   float *KW2 = nullptr;
   float2 *tw = nullptr;
+  // hydro kernel: the tiled form (hydro32t.cuh) unless DISKGPU_HYDRO32=warp selects the
+  // warp-marching form (hydro32w.cuh); both compute the same step
+  bool hydro_tile = true;
   // A = 32 (Nu = 1024): the four u passes run as one fused kernel (uconv.cuh)
   bool fused_u = false;
   float *khm = nullptr;  // khat[m][p] / M, [nm][M]
@@ -79,6 +85,18 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // K-major BF16 matrix [rows][cols] -> tiles of box_rows x 64 with 128-byte swizzle.
+// every instantiation of the tiled hydro kernel takes more than 48 KB of shared memory
+static cudaError_t hydro32t_prepare() {
+  const void *fns[] = {(const void *)k_hydro32t<true, kForcePhi>, (const void *)k_hydro32t<false, kForcePhi>,
+                       (const void *)k_hydro32t<true, kForceArrays>, (const void *)k_hydro32t<false, kForceArrays>,
+                       (const void *)k_hydro32t<true, kForceNone>, (const void *)k_hydro32t<false, kForceNone>};
+  for (const void *f : fns) {
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem32t);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 // radial-direction layout of the split-BF16 gravity: factored (M = 2 Nu = 64 x Nu/32) when
 // Nu is a multiple of 1024, and the four factored passes fused into one kernel at Nu = 1024
 static bool u_factored(int Nu) { return Nu % 1024 == 0; }
@@ -400,6 +418,24 @@ static void free_split(SplitBuf &b) {
   b.hi = b.lo = nullptr;
 }
 
+// Launch with programmatic stream serialization: the kernel may begin (its prologue up to
+// pdl_wait) while the previous kernel on the stream drains.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 template <int MODE, bool A_MN = false, bool B_MN = false>
 static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUtensorMap &Bh, const CUtensorMap &Bl,
                         int M, int N, int K, const tc::GemmArgs &base, cudaStream_t st) {
@@ -410,14 +446,14 @@ static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUte
   // short contractions (one or two K chunks) need no deep pipeline: fewer stages let more
   // CTAs share an SM and hide each tile's load / epilogue latency
   const int nk = K / tc::BK;
-  if (nk <= 1) {
-    tc::k_gemm_split<MODE, A_MN, B_MN, 1><<<grid, tc::kThreads, tc::smem_bytes(1), st>>>(Ah, Al, Bh, Bl, a);
-  } else if (nk <= 2) {
-    tc::k_gemm_split<MODE, A_MN, B_MN, 2><<<grid, tc::kThreads, tc::smem_bytes(2), st>>>(Ah, Al, Bh, Bl, a);
-  } else {
-    tc::k_gemm_split<MODE, A_MN, B_MN, tc::STAGES><<<grid, tc::kThreads, tc::smem_bytes(tc::STAGES), st>>>(Ah, Al, Bh, Bl, a);
-  }
-  return cudaGetLastError();
+  if (nk <= 1)
+    return launch_pdl(tc::k_gemm_split<MODE, A_MN, B_MN, 1>, grid, dim3(tc::kThreads), tc::smem_bytes(1), st, Ah, Al,
+                      Bh, Bl, a);
+  if (nk <= 2)
+    return launch_pdl(tc::k_gemm_split<MODE, A_MN, B_MN, 2>, grid, dim3(tc::kThreads), tc::smem_bytes(2), st, Ah, Al,
+                      Bh, Bl, a);
+  return launch_pdl(tc::k_gemm_split<MODE, A_MN, B_MN, tc::STAGES>, grid, dim3(tc::kThreads),
+                    tc::smem_bytes(tc::STAGES), st, Ah, Al, Bh, Bl, a);
 }
 
 // The smem limit of every instantiation gemm() may launch, raised once at set-up.
@@ -532,6 +568,11 @@ int dg_handle::mixed_init() {
   XK((prepare_gemm<tc::kEpiSplitScaled, false, false>()));
   XK((prepare_gemm<tc::kEpiRowScaleF32, false, false>()));
   XK(cudaStreamSynchronize(st));
+  {
+    const char *hk = getenv("DISKGPU_HYDRO32");
+    X.hydro_tile = !(hk && strcmp(hk, "warp") == 0) && Nphi >= kLd32t;
+    if (X.hydro_tile) XK(hydro32t_prepare());
+  }
   X.tables_ready = true;
   return DG_OK;
 }
@@ -704,6 +745,19 @@ int dg_handle::mixed_download_state(double *Sig, double *vRh, double *vph) {
 static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *u, const float *w, const float *Phi,
                                   const double *gR, const double *gp, int fm, float *so, float *uo, float *wo, Ctl *ctl,
                                   cudaStream_t st) {
+  if (X.hydro_tile) {
+    dim3 grid((X.Nphi + kTileJ - 1) / kTileJ, (X.Nu + kTileI - 1) / kTileI);
+    const SplitBf16 sx{X.Sx.hi, X.Sx.lo};
+    cudaError_t e = cudaSuccess;
+    auto go = [&](auto kern) {
+      e = launch_pdl(kern, grid, dim3(kThreads32t), kSmem32t, st, sig, u, w, Phi, gR, gp, so, uo, wo, sx, ctl, X.rows);
+    };
+    const bool g2 = X.rows.gamma2 != 0;
+    if (fm == kForcePhi) g2 ? go(k_hydro32t<true, kForcePhi>) : go(k_hydro32t<false, kForcePhi>);
+    else if (fm == kForceArrays) g2 ? go(k_hydro32t<true, kForceArrays>) : go(k_hydro32t<false, kForceArrays>);
+    else g2 ? go(k_hydro32t<true, kForceNone>) : go(k_hydro32t<false, kForceNone>);
+    return e;
+  }
   const int nstrips = (X.Nphi + kOutCols32 - 1) / kOutCols32;
   dim3 grid((nstrips + kWarps32 - 1) / kWarps32, (X.Nu + kBand32 - 1) / kBand32);
   k_hydro32w<<<grid, kWarps32 * 32, 0, st>>>(sig, u, w, Phi, gR, gp, fm, so, uo, wo, SplitBf16{X.Sx.hi, X.Sx.lo}, ctl,
@@ -730,9 +784,8 @@ int dg_handle::mixed_gravity() {
     if (X.fused_u) {
       // F1, F2, I1, I2 in one kernel: four modes per CTA, operands kept on chip
       tc::UconvArgs u{X.twp, X.khm, X.Z.hi, X.Z.lo, Nu, Nphi, &ctl->status};
-      tc::k_uconv<<<nm / tc::kUcModes, tc::kUcThreads, tc::kUcSmem, st>>>(
-          X.mRB[0], X.mRB[1], X.mXin[0], X.mXin[1], X.mRA[0], X.mRA[1], X.mRGA[0], X.mRGA[1], X.mRGB[0], X.mRGB[1], u);
-      XK(cudaGetLastError());
+      XK(launch_pdl(tc::k_uconv, dim3(nm / tc::kUcModes), dim3(tc::kUcThreads), tc::kUcSmem, st, X.mRB[0], X.mRB[1],
+                    X.mXin[0], X.mXin[1], X.mRA[0], X.mRA[1], X.mRGA[0], X.mRGA[1], X.mRGB[0], X.mRGB[1], u));
     } else {
       // F1: 64-point DFT over i2 (K = 32 complex), twiddle, -> Tb[(i1, ri)][(m, p2)]
       a.out_hi = X.Tb.hi; a.out_lo = X.Tb.lo;

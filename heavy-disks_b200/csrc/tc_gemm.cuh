@@ -297,6 +297,8 @@ __global__ void __launch_bounds__(kThreads, (NS == 1 ? 4 : (NS == 2 ? 2 : 1)))
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_d = tmem_slot;
+  pdl_wait();  // operands come from the previous kernel on the stream
+  pdl_trigger();
 
   if (warp == 0 && lane == 0) {
     // ---- TMA producer ----

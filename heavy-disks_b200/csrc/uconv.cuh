@@ -128,15 +128,11 @@ __global__ void __launch_bounds__(kUcThreads, 1)
   const float2 *tws = reinterpret_cast<const float2 *>(sm + kUcTw);
 
   if (threadIdx.x == 0) {
+    // constant tables first: they do not depend on the previous kernel
     mbar_arrive_expect_tx(&bar_in0, 65536 + kUcTwBytes);
     bulk_load(sm + kUcTw, a.twiddle, kUcTwBytes, &bar_in0);
     tma_load_2d(sm + kUcRB, &tRBh, &bar_in0, 0, 0);
     tma_load_2d(sm + kUcRB + 16384, &tRBl, &bar_in0, 0, 0);
-    const int x0 = blockIdx.x * (kUcModes * 32);
-    tma_load_2d(sm + kUcX, &tXh, &bar_in0, x0, 0);
-    tma_load_2d(sm + kUcX + 8192, &tXh, &bar_in0, x0 + 64, 0);
-    tma_load_2d(sm + kUcX + 16384, &tXl, &bar_in0, x0, 0);
-    tma_load_2d(sm + kUcX + 24576, &tXl, &bar_in0, x0 + 64, 0);
     mbar_arrive_expect_tx(&bar_in1, 65536);
     tma_load_2d(sm + kUcRA, &tRAh, &bar_in1, 0, 0);
     tma_load_2d(sm + kUcRA + 8192, &tRAl, &bar_in1, 0, 0);
@@ -146,6 +142,13 @@ __global__ void __launch_bounds__(kUcThreads, 1)
     tma_load_2d(sm + kUcRGB + 8192, &tRGBh, &bar_in1, 64, 0);
     tma_load_2d(sm + kUcRGB + 16384, &tRGBl, &bar_in1, 0, 0);
     tma_load_2d(sm + kUcRGB + 24576, &tRGBl, &bar_in1, 64, 0);
+    // the phi spectrum is the previous kernel's output
+    pdl_wait();
+    const int x0 = blockIdx.x * (kUcModes * 32);
+    tma_load_2d(sm + kUcX, &tXh, &bar_in0, x0, 0);
+    tma_load_2d(sm + kUcX + 8192, &tXh, &bar_in0, x0 + 64, 0);
+    tma_load_2d(sm + kUcX + 16384, &tXl, &bar_in0, x0, 0);
+    tma_load_2d(sm + kUcX + 24576, &tXl, &bar_in0, x0 + 64, 0);
     // ---- S1: D1[(p2, ro)][(m, i1)] at TMEM columns 0..127 ----
     in0_seen = mbar_wait(&bar_in0, 0, a.status);
     if (in0_seen) {
@@ -161,6 +164,8 @@ __global__ void __launch_bounds__(kUcThreads, 1)
     }
   }
   __syncwarp();
+  pdl_wait();  // every thread: Z is read by the kernel after this one's predecessor
+  pdl_trigger();
   bool ok = mbar_wait(&bar_mma, 0, a.status);
   tc_fence_after();
 
