@@ -35,3 +35,31 @@ def saturation_ratio(c0, c2, tail=8):
     c0 = np.asarray(c0, dtype=np.float64)[-tail:]
     c2 = np.asarray(c2, dtype=np.float64)[-tail:]
     return float(np.mean(c2 / c0))
+
+
+def linear_phase(t, c0, c2, arg2, t0=1.0, ratio_end=0.05):
+    """gamma, Omega_p of the exponential phase: records from t0 (past the seed's transient)
+    until |C2|/|C0| first exceeds ratio_end (the mode is still linear there).
+    Returns (gamma, omega_p, n_points)."""
+    t = np.asarray(t, dtype=np.float64)
+    ratio = np.asarray(c2, dtype=np.float64) / np.asarray(c0, dtype=np.float64)
+    hit = np.flatnonzero(ratio > ratio_end)
+    tend = t[hit[0]] if len(hit) else t[-1]
+    sel = (t >= t0) & (t <= tend)
+    if sel.sum() < 4:
+        sel = t >= 0.5 * t0
+    return fit_growth(t[sel], np.asarray(c2)[sel], np.asarray(arg2)[sel])
+
+
+def saturated_phase(t, c0, c2, arg2, ratio_min=0.15):
+    """Mean |C2|/|C0| and pattern speed over the records where the mode has saturated
+    (|C2|/|C0| >= ratio_min, from its first crossing to its last).  Returns
+    (ratio, omega_p, n_points)."""
+    t = np.asarray(t, dtype=np.float64)
+    ratio = np.asarray(c2, dtype=np.float64) / np.asarray(c0, dtype=np.float64)
+    hit = np.flatnonzero(ratio >= ratio_min)
+    if len(hit) < 2:
+        raise ValueError("the mode never saturated above ratio_min")
+    sel = slice(hit[0], hit[-1] + 1)
+    _, w, n = fit_growth(t[sel], np.asarray(c2)[sel], np.asarray(arg2)[sel])
+    return float(np.mean(ratio[sel])), w, n

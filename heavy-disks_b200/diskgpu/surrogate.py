@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 import json
+import os
 
 import numpy as np
 
@@ -112,24 +113,60 @@ class Surrogate:
         y = self.net.forward(self._norm(X)).astype(np.float64)
         return y * self.ys + self.ym
 
-    def save(self, path):
+    def save(self, path, report=None):
+        """Write the network and its standardisation: .npz (compressed, float32 parameters)
+        or .json."""
+        if str(path).endswith(".npz"):
+            np.savez_compressed(path, shape=np.array(self.net.shape, dtype=np.int64), params=self.net.params(),
+                                xm=self.xm, xs=self.xs, ym=self.ym, ys=self.ys,
+                                report=np.array(json.dumps(report or {})))
+            return
         with open(path, "w") as f:
-            json.dump({"shape": self.net.shape, "params": self.net.params().tolist(),
-                       "xm": self.xm.tolist(), "xs": self.xs.tolist(), "ym": self.ym.tolist(),
-                       "ys": self.ys.tolist()}, f)
+            json.dump({"shape": list(self.net.shape), "params": self.net.params().tolist(), "xm": self.xm.tolist(),
+                       "xs": self.xs.tolist(), "ym": self.ym.tolist(), "ys": self.ys.tolist()}, f)
 
     @classmethod
     def load(cls, path, device=-1):
-        with open(path) as f:
-            d = json.load(f)
-        s = cls(width=d["shape"][1], depth=d["shape"][2], device=device)
-        s.net.set_params(np.array(d["params"], dtype=np.float32))
-        s.xm, s.xs = np.array(d["xm"]), np.array(d["xs"])
-        s.ym, s.ys = np.array(d["ym"]), np.array(d["ys"])
+        d = read_surrogate(path)
+        s = cls(width=int(d["shape"][1]), depth=int(d["shape"][2]), device=device)
+        s.net.set_params(np.asarray(d["params"], dtype=np.float32))
+        s.xm, s.xs, s.ym, s.ys = d["xm"], d["xs"], d["ym"], d["ys"]
         return s
 
 
+def read_surrogate(path):
+    """The stored surrogate as plain arrays: shape, params (float32), xm, xs, ym, ys, report."""
+    if str(path).endswith(".npz"):
+        with np.load(path) as z:
+            return {"shape": [int(v) for v in z["shape"]], "params": z["params"].astype(np.float32),
+                    "xm": z["xm"], "xs": z["xs"], "ym": z["ym"], "ys": z["ys"],
+                    "report": json.loads(str(z["report"])) if "report" in z else {}}
+    with open(path) as f:
+        d = json.load(f)
+    return {"shape": d["shape"], "params": np.array(d["params"], dtype=np.float32), "xm": np.array(d["xm"]),
+            "xs": np.array(d["xs"]), "ym": np.array(d["ym"]), "ys": np.array(d["ys"]), "report": {}}
+
+
+# The surrogate trained on the sweep law with the package's own batched hydro (report inside
+# the file), shipped with the package.
+TRAINED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "surrogate.npz")
+
+
+def lka98_features(mstar=0.6, mdisk=0.4, Qmin=1.27, soft_over_r=0.05, gamma=2.0):
+    """Surrogate inputs (Q_min, M_d/M_*, softening/r, Gamma) of an LKA98 disk.  The standard
+    disk (lka98/model.py: m* = 0.6, m_D = 0.4; Q_min = 1.27 by lka98/EQUATIONS.md; Gamma = 2)
+    is softened by ~0.02 r at its density peak, below the trained range, so the lowest
+    trained value 0.05 stands in for it."""
+    return np.array([[Qmin, mdisk / mstar, soft_over_r, gamma]])
+
+
 def lka98_omega_guess(pred_gamma, pred_omega_p, m=2):
-    """Seed for lka98.eigensolve.solve_mode: omega = m Omega_p - i gamma (the convention of
-    lka98/eigensolve.py:153, where 3.15057 - 0.72278i means Omega_p = 1.5753, gamma = 0.7228)."""
+    """Seed for lka98.eigensolve: omega = m Omega_p - i gamma (the convention of
+    lka98/eigensolve.py:153, where 3.15057 - 0.72278i means Omega_p = 1.5753, gamma = 0.7228).
+
+    The hydro's disks differ from the linear model (softening, finite amplitude), so the seed
+    is the centre of a coarse contour rather than a Newton start: lka98's
+    contour_root(problem, seed, 0.35, 0.35, n=16) followed by solve_mode(problem, root,
+    localize=False) finds the growing mode with 4 x 16 + a few dlogdet calls instead of the
+    default 4 x 160 + a few."""
     return complex(m * pred_omega_p, -pred_gamma)

@@ -5,8 +5,8 @@
 Draws sweep points with the sweep law (diskgpu.sweep.draw, fixed seed), runs them in
 batches of disks advanced together (dg_batch, mixed precision), fits gamma / Omega_p /
 saturated |C2|/|C0| from each disk's mode records, trains the MLP on 95 % and reports its
-error on the 5 % held out (the hydro is the judge).  Writes dataset.npz, surrogate.json
-and report.json to --out.
+error on the 5 % held out against the hydro's own values.  Writes dataset.npz,
+surrogate.npz (network, standardisation and report) and report.json to --out.
 """
 from __future__ import annotations
 
@@ -19,20 +19,16 @@ import numpy as np
 
 from . import MIXED, Batch, params_physical
 from . import sweep as S
-from .analysis import fit_growth
+from .analysis import linear_phase
 from .surrogate import Surrogate
 
 
 def fit_record(rec):
-    """gamma / Omega_p over the linear phase and the saturated ratio of one disk."""
+    """gamma / Omega_p over the linear phase and the late-time |C2|/|C0| of one disk (mean of
+    the last quarter of its records)."""
     t, c0, c2, a2 = rec[:, 0], rec[:, 1], rec[:, 2], rec[:, 3]
+    g, w, _ = linear_phase(t, c0, c2, a2)
     ratio = c2 / c0
-    sat = np.flatnonzero(ratio > 0.05)
-    tend = t[sat[0]] if len(sat) else t[-1]
-    sel = (t >= 1.0) & (t <= tend)
-    if sel.sum() < 4:
-        sel = t >= 0.5
-    g, w, _ = fit_growth(t[sel], c2[sel], a2[sel])
     tail = ratio[-max(4, len(ratio) // 4):]
     return g, w, float(np.mean(tail))
 
@@ -95,7 +91,7 @@ def main():
         "target_std": dict(zip(["gamma", "omega_p", "sat_ratio"], Y.std(axis=0).tolist())),
         "loss_first_last": [hist[0], hist[-1]],
     }
-    sur.save(os.path.join(a.out, "surrogate.json"))
+    sur.save(os.path.join(a.out, "surrogate.npz"), report=rep)
     with open(os.path.join(a.out, "report.json"), "w") as f:
         json.dump(rep, f, indent=1)
     print(json.dumps(rep))

@@ -13,6 +13,7 @@ test_kalnajs.cpp), compiled unmodified against the project's FFTW shim by
 Needs the reference tree (only present where the fixtures are generated); the tests
 read only the committed outputs.  Usage: python tests/golden/make_golden.py
 """
+import argparse
 import os
 import shutil
 import subprocess
@@ -38,25 +39,40 @@ CASES = {
 DISKDISK = {
     # name: argv of diskdisk (Nu Nphi eps tlim selfgrav amp nthreads)
     "64_t1": ["64", "64", "0.01", "1.0", "1", "1e-3", "1"],
+    # the growth-rate-versus-softening runs of diskfft/README.md:25-27 (128^2, to t = 9)
+    "128_e0.02_t9": ["128", "128", "0.02", "9", "1", "1e-3", "8"],
+    "128_e0.005_t9": ["128", "128", "0.005", "9", "1", "1e-3", "8"],
+    "128_e0.0025_t9": ["128", "128", "0.0025", "9", "1", "1e-3", "8"],
+    # through saturation (README.md:41-42 quotes |C2|/|C0| = 0.24, Omega_p 1.46 -> 1.34)
+    "256_e0.005_t20": ["256", "256", "0.005", "20", "1", "1e-3", "8"],
 }
 
 
 def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", nargs="*", help="regenerate only these fixtures (names above)")
+    a = ap.parse_args()
+    want = (lambda n: True) if not a.only else (lambda n: n in a.only)
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", "ref"], check=True)
     ref = os.path.join(ROOT, "oracle", "_ref")
     tmp = os.path.join(HERE, "_tmp")
     os.makedirs(tmp, exist_ok=True)
     for name, (Nu, Nphi, eps, sg, amp, n) in CASES.items():
+        if not want(name):
+            continue
         out = os.path.join(tmp, name + ".bin")
         subprocess.run([os.path.join(ref, "refdump"), str(Nu), str(Nphi), repr(eps), str(sg),
                         repr(amp), str(n), out], check=True)
         r = O.read_refdump(out)
         np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), **{k: np.asarray(v) for k, v in r.items()})
-    res = subprocess.run([os.path.join(ref, "test_kalnajs_ref")], capture_output=True, text=True)
-    with open(os.path.join(HERE, "test_kalnajs_ref.txt"), "w") as f:
-        f.write(res.stdout)
-        f.write(f"exit={res.returncode}\n")
+    if want("test_kalnajs_ref"):
+        res = subprocess.run([os.path.join(ref, "test_kalnajs_ref")], capture_output=True, text=True)
+        with open(os.path.join(HERE, "test_kalnajs_ref.txt"), "w") as f:
+            f.write(res.stdout)
+            f.write(f"exit={res.returncode}\n")
     for name, argv in DISKDISK.items():
+        if not want(name):
+            continue
         d = os.path.join(HERE, f"diskdisk_ref_{name}")
         os.makedirs(d, exist_ok=True)
         res = subprocess.run([os.path.join(ref, "diskdisk_ref")] + argv, capture_output=True, text=True,

@@ -66,3 +66,19 @@ def test_training_fits_a_smooth_map():
     xv, tv = _data(512, seed=9)
     err = np.sqrt(np.mean((s.predict(xv) - tv) ** 2, axis=0)) / t.std(axis=0)
     assert np.all(err < 0.2)
+
+
+def test_shipped_surrogate_on_gpu_matches_oracle():
+    """The shipped network, loaded onto the GPU, predicts what the FP64 oracle predicts for
+    its parameters (held-out sweep points and the LKA98 standard disk)."""
+    import os
+
+    from diskgpu.surrogate import TRAINED, lka98_features, read_surrogate
+    d = read_surrogate(TRAINED)
+    with np.load(os.path.join(os.path.dirname(TRAINED), "sweep_128_dataset.npz")) as z:
+        X = np.concatenate([z["data"][-51:, :4], lka98_features()])
+    sur = Surrogate.load(TRAINED)
+    got = sur.predict(X)
+    ref = np.asarray(R.forward(d["params"].astype(np.float64), (X - d["xm"]) / d["xs"], *d["shape"])) * d["ys"] + d["ym"]
+    assert np.max(np.abs(got - ref) / d["ys"]) <= 1e-3
+    sur.net.close()
