@@ -12,6 +12,9 @@ The K timed steps run as dg_run_steps calls of --chunk steps (each one launch of
 captured step loop, the way dg_advance runs a disk), with L2 flushed before every call and
 CUDA events around it.  Then --cold-steps single steps, each after an L2 flush, give the
 cold per-step time and, with per-kernel events, the roofline of every kernel of the step.
+On one GPU the line also carries `fp64_same_disk` (the plain FP64 path on the same disk,
+timed the same way, and the mixed/FP64 ratio the metric names) and `batched_sweep` (256
+disks of the sweep law, grids 128^2..512^2, advanced together by dg_batch).
 
 --impl reference times the reference's own CPU implementation (diskfft/src hydro.hpp +
 kalnajs.hpp compiled unmodified against the FFTW-API shim, oracle/_ref/refbench) on the
@@ -49,6 +52,11 @@ def parse():
     ap.add_argument("--chunk", type=int, default=64, help="steps per timed iteration (one graph launch)")
     ap.add_argument("--cold-steps", type=int, default=200,
                     help="single steps with a flushed L2, timed and profiled per kernel")
+    ap.add_argument("--fp64-steps", type=int, default=1024,
+                    help="steps of the plain FP64 path on the same disk (0: skip the comparison)")
+    ap.add_argument("--batch-disks", type=int, default=256,
+                    help="disks of the batched sweep measurement (0: skip it)")
+    ap.add_argument("--batch-tlim", type=float, default=0.1, help="time the batched sweep advances")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -234,6 +242,72 @@ def gravity_parts(precision, Nu, Nphi):
             ("grav_phi_inv", "inverse phi DFT GEMM + potential scaling (k_gemm_split)", "tensor", g4, "flop")]
 
 
+def timed_chunks(disk, stream, flush, steps, chunk):
+    """Device milliseconds of `steps` steps of `disk` run as dg_run_steps calls of `chunk`
+    steps (after 3 untimed calls), with L2 flushed before every call and CUDA events
+    around each."""
+    import torch
+    chunk = max(1, min(chunk, steps))
+    sizes = [chunk] * (steps // chunk) + ([steps % chunk] if steps % chunk else [])
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            flush.zero_()
+            disk.run_steps(chunk, 0.3, sync=False)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in sizes]
+        for k, n in enumerate(sizes):
+            flush.zero_()
+            ev[k][0].record(stream)
+            disk.run_steps(n, 0.3, sync=False)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    disk.run_steps(0, 0.3, sync=True)
+    return sum(b.elapsed_time(e) for b, e in ev)
+
+
+def fp64_same_disk(a, device, stream, flush, phase0):
+    """The plain FP64 path (the reference's arithmetic) on the same disk, timed the same way."""
+    import diskgpu as D
+    N = a.size
+    with D.Disk(N, N, eps=a.eps, amp=1e-3, precision="fp64", phase0=phase0, device=device) as d:
+        d.init_standard()
+        d.set_stream(stream.cuda_stream)
+        ms = timed_chunks(d, stream, flush, a.fp64_steps, a.chunk)
+    return {"value": N * N * a.fp64_steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / a.fp64_steps,
+            "steps": a.fp64_steps, "how": "same disk and timing as the headline, precision fp64 (k_hydro64 + "
+                                          "three shared-memory FFT passes)"}
+
+
+def batched_sweep(a, device):
+    """Throughput of a batched sweep: `--batch-disks` disks drawn by the sweep law (grids
+    128^2..512^2, Q_min, M_d/M_*, softening/r, Gamma; seed 12345), mixed precision, advanced
+    together by dg_batch (one graph launch advances every disk 64 steps)."""
+    import torch
+    import diskgpu as D
+    from diskgpu import sweep as S
+    pts = S.draw(a.batch_disks, seed=12345, grids=(128, 256, 384, 512))
+    params = []
+    for pt in pts:
+        p, _ = D.params_physical(pt.Qmin, pt.mass_ratio, pt.soft_over_r, pt.gamma)
+        p.Nu = p.Nphi = pt.N
+        p.amp, p.phase0, p.precision, p.device = 1e-3, pt.phase0, D.MIXED, device
+        params.append(p)
+    with D.Batch(params) as b:
+        b.init_standard()
+        _, _, s0 = b.advance(0.01, steps_per_launch=64)  # captures the graph
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, _, s1 = b.advance(0.01 + a.batch_tlim, steps_per_launch=64)
+        el = time.perf_counter() - t0
+    zu = float(sum(pt.N * pt.N * (int(x1) - int(x0)) for pt, x0, x1 in zip(pts, s0, s1)))
+    grids = {}
+    for pt in pts:
+        grids[pt.N] = grids.get(pt.N, 0) + 1
+    return {"value": zu / el, "unit": UNIT, "disks": len(pts), "grids": {f"{k}^2": v for k, v in sorted(grids.items())},
+            "zone_updates": zu, "seconds": el, "sim_time": a.batch_tlim,
+            "how": "wall clock around dg_batch_advance (graph launches of 64 steps per disk, the host reads "
+                   "every disk's control block between launches)"}
+
+
 TRAFFIC_KEYS = {"hydro": "hydro", "grav_phi_fwd": "grav_phi_fwd", "grav_u": "grav_u", "grav_phi_inv": "grav_phi_inv"}
 
 
@@ -384,6 +458,15 @@ def main():
             dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
             e2e["value"] = world * zones * a.e2e_steps / float(t_e.item())
 
+    # ---- the plain FP64 path on the same disk, and a batched sweep (one rank) ----
+    fp64 = batch = None
+    if world == 1 and a.precision == "mixed":
+        if a.fp64_steps > 0:
+            fp64 = fp64_same_disk(a, local, stream, flush, phase0)
+            fp64["mixed_over_fp64"] = value / fp64["value"]
+        if a.batch_disks > 0:
+            batch = batched_sweep(a, local)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_sample(N, a.eps)
@@ -408,6 +491,7 @@ def main():
             "data": "synthetic (standard heavy disk, seeded m=2 phase)", "config": cfg,
             "roofline": roof, "roofline_all": roof_all, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": kps * a.steps, "clocks": clk.summary(),
+            "fp64_same_disk": fp64, "batched_sweep": batch,
         }
         print(json.dumps(line))
     disk.close()
