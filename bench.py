@@ -482,7 +482,7 @@ def main():
                     "cold_l2_single_step": {"ms_per_step": cold_ms, "steps": cold_n,
                                             "note": "one step per timed iteration, L2 flushed before each"},
                     "stream": "caller stream via dg_set_stream", "phase_share_cold": share,
-                    "kernels_per_step": kps})
+                    "kernels_per_step": kps, "autotuner": disk.tuning()})
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": warm_iters * chunk, "ms_per_step": ms_max / a.steps, "higher_is_better": True,

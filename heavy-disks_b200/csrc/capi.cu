@@ -787,6 +787,13 @@ int dg_profile_enable(dg_handle *h, int on) {
   return DG_OK;
 }
 
+int dg_tuning_info(const dg_handle *h, char *buf, int len) {
+  if (!h || !buf || len < 1) return DG_ERR_INVALID;
+  const std::string s = h->p.precision == DG_PREC_MIXED ? h->mixed_tuning_info() : std::string("fp64: one variant per kernel");
+  snprintf(buf, (size_t)len, "%s", s.c_str());
+  return DG_OK;
+}
+
 int dg_kernels_per_step(const dg_handle *h) {
   if (!h) return DG_ERR_INVALID;
   const int grav = !h->p.selfgrav ? 0 : (h->p.precision == DG_PREC_MIXED ? h->mixed_gravity_kernels() : 3);

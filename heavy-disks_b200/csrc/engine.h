@@ -95,6 +95,8 @@ struct dg_handle {
   int mixed_download_state(double *Sig, double *vR, double *vp);
   int mixed_gravity();
   int mixed_gravity_kernels() const;
+  int mixed_autotune();
+  std::string mixed_tuning_info() const;
   int mixed_potential(const double *dSig, double *dOut);
   bool in_step_host = false;  // upload from dg_step_host keeps the mixed basic state
   void mixed_basic(std::vector<double> *S0, std::vector<double> *V0, std::vector<double> *g0) const;

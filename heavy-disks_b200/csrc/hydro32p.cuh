@@ -1,0 +1,466 @@
+// Packed form of the tiled mixed-precision hydro step: the same stages, shared-memory plan
+// and arithmetic as hydro32t.cuh, with every thread advancing two adjacent columns at once
+// in FP32x2 registers (Blackwell's paired FADD2 / FMUL2 / FFMA2), so one instruction, one
+// shared-memory access and one set of row constants serve two zones.
+//
+// Tile: kTileI rows x kTileJp = 56 output columns, stored columns c = j - (j0 - 4) in
+// [0, 64) (a 4-column halo on each side keeps every column pair, and every global pair
+// access, 8-byte aligned, also across the periodic wrap).  Lane l of a warp owns the pair
+// (2l, 2l+1) of every row it visits; warp w visits rows w, w + 8, ...  Azimuthal
+// neighbours (columns 2l - 2 .. 2l + 2) come from the neighbouring lanes by shuffle.
+// Columns whose results are never used (lanes 0 and 31 in the sweeps) are computed
+// anyway and discarded, so shuffles run with every lane active.
+#pragma once
+
+#include "hydro32t.cuh"
+
+namespace dg {
+
+constexpr int kTileJp = kLd32t - 8;        // output columns per CTA (56)
+constexpr int kWarps32p = kThreads32t / 32;  // 8 row groups, one warp each
+constexpr int kItLoadP = (kRows32t + kWarps32p - 1) / kWarps32p;
+constexpr int kItSrcP = (kSrcRows32t + kWarps32p - 1) / kWarps32p;
+constexpr int kItFaceP = (kFaceRows32t + kWarps32p - 1) / kWarps32p;
+constexpr int kItOutP = (kTileI + kWarps32p - 1) / kWarps32p;
+static_assert(kItOutP * kWarps32p == kTileI, "output rows split evenly over the warps");
+
+namespace p2 {
+typedef float2 F2;
+__device__ __forceinline__ F2 S(float a) { return make_float2(a, a); }
+__device__ __forceinline__ F2 add(F2 a, F2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ F2 mul(F2 a, F2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ F2 fma(F2 a, F2 b, F2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ F2 sub(F2 a, F2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }  // exact a - b
+__device__ __forceinline__ F2 sel(bool px, bool py, F2 a, F2 b) {
+  return make_float2(px ? a.x : b.x, py ? a.y : b.y);
+}
+__device__ __forceinline__ F2 sels(bool px, bool py, float a, float b) {
+  return make_float2(px ? a : b, py ? a : b);
+}
+__device__ __forceinline__ F2 fdiv(F2 a, F2 b) { return make_float2(__fdividef(a.x, b.x), __fdividef(a.y, b.y)); }
+// hydro.hpp:16-18 on each half (see vanleer32)
+__device__ __forceinline__ F2 vanleer(F2 a, F2 b) {
+  const F2 p = mul(a, b), s = add(a, b), n = add(p, p);
+  return make_float2(p.x > 0.f ? __fdividef(n.x, s.x) : 0.f, p.y > 0.f ? __fdividef(n.y, s.y) : 0.f);
+}
+__device__ __forceinline__ float up1(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ float dn1(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+}  // namespace p2
+
+template <bool G2, int FM, bool IN>
+__device__ __forceinline__ void hydro32p_tile(
+    const float *__restrict__ sig, const float *__restrict__ uu, const float *__restrict__ ww,
+    const float *__restrict__ Phi, const double *__restrict__ gRin, const double *__restrict__ gpin,
+    float *__restrict__ so, float *__restrict__ uo, float *__restrict__ wo, const SplitBf16 &Sx, Ctl *ctl,
+    const Rows32 &g, float *sm32t, double *red, double *bsum, double *zsum) {
+  using namespace p2;
+  float *rc = sm32t + kOffRc32t;
+  // shared arrays as pairs: row r, lane l -> element r * 32 + l
+  constexpr int L2 = kLd32t / 2;
+  F2 *SG = reinterpret_cast<F2 *>(sm32t + kOffSg32t), *DP = reinterpret_cast<F2 *>(sm32t + kOffDp32t);
+  F2 *PH = reinterpret_cast<F2 *>(sm32t + kOffPh32t);
+  F2 *U1 = reinterpret_cast<F2 *>(sm32t + kOffU132t), *W1 = reinterpret_cast<F2 *>(sm32t + kOffW132t);
+  F2 *FF = reinterpret_cast<F2 *>(sm32t + kOffF32t), *FR = FF + kFaceArr32t / 2, *GA = FR + kFaceArr32t / 2,
+     *GB = GA + kFaceArr32t / 2;
+  F2 *U2 = DP, *W2 = PH;            // S4 outputs over the dead source inputs
+  F2 *PF = FF, *PR = FR, *PG = GA;  // S5 outputs over the dead radial fluxes
+  F2 *S3 = U1;                      // new sigma for the mode sums
+
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  const int Nu = g.Nu, Nphi = g.Nphi;
+  const int i0 = blockIdx.y * kTileI, j0 = blockIdx.x * kTileJp;
+  const int ib = i0 - 3;
+  const int iend = (i0 + kTileI < Nu) ? i0 + kTileI : Nu;
+  const int jc = wrap_col(j0 - 4 + 2 * lane, Nphi);  // global column of this lane's first element (even)
+  // output columns c in [4, 60): lanes 2..29, each element inside the grid
+  const bool out_lane = lane >= 2 && lane < 2 + kTileJp / 2;
+  const bool outx = out_lane && j0 + 2 * lane - 4 < Nphi, outy = out_lane && j0 + 2 * lane - 3 < Nphi;
+#define RC(k, i) rc[(k) * kRows32t + (i) - ib]
+  auto row_ok = [&](int i) { return IN || (i >= 0 && i < Nu); };
+  auto first_row = [&](int i) { return !IN && i == 0; };
+  auto last_row = [&](int i) { return !IN && i == Nu - 1; };
+
+  for (int t = tid; t < tNConst * kRows32t; t += kThreads32t) {
+    const int k = t / kRows32t, r = t - k * kRows32t, i = ib + r;
+    float v = 0.f;
+    if (i >= 0 && i <= Nu) {
+      const bool row = i < Nu;
+      switch (k) {
+        case tS0: v = row ? g.S0[i] : 0.f; break;
+        case tInvS0: v = row ? g.invS0[i] : 0.f; break;
+        case tV0: v = row ? g.V0[i] : 0.f; break;
+        case tA0: v = row ? g.a0[i] : 0.f; break;
+        case tDP0: v = row ? g.dP0dR[i] : 0.f; break;
+        case tInvdRc: v = row ? g.invdRc[i] : 0.f; break;
+        case tInvR: v = row ? g.invR[i] : 0.f; break;
+        case tR: v = row ? g.R[i] : 0.f; break;
+        case tInvVol: v = row ? g.invVol[i] : 0.f; break;
+        case tInvdl: v = row ? g.invdl[i] : 0.f; break;
+        case tAphi: v = row ? g.Aphi[i] : 0.f; break;
+        case tR32: v = row ? g.R32[i] : 0.f; break;
+        case tInvdR: v = row ? g.invdR[i] : 0.f; break;
+        case tP0: v = row ? g.P0[i] : 0.f; break;
+        case tDS0: v = g.dS0[i]; break;
+        case tDV: v = g.dV[i]; break;
+        case tAf: v = g.Af[i]; break;
+        case tInvdRl: v = g.invdRl[i]; break;
+        case tInvdRr: v = g.invdRr[i]; break;
+      }
+    }
+    rc[t] = v;
+  }
+  if (tid < 2 * kMaxModes) {
+    bsum[tid] = 0.0;
+    zsum[tid] = 0.0;
+  }
+  pdl_wait();  // dt, the state and dPhi come from earlier kernels on the stream
+  pdl_trigger();
+  const StepInfo si = read_step_info(ctl, true);
+  const float dt = (float)si.dt;
+  float lmaxf = 0.f;
+  bool bad = false;
+
+  if (!si.active) {
+    // pass-through: copy the tile and report the CFL rate of the unchanged state
+#pragma unroll
+    for (int k = 0; k < kItOutP; ++k) {
+      const int i = i0 + wp + kWarps32p * k;
+      if (i < Nu) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          if (e == 0 ? outx : outy) {
+            const size_t q = (size_t)i * Nphi + jc + e;
+            so[q] = sig[q]; uo[q] = uu[q]; wo[q] = ww[q];
+            lmaxf = fmaxf(lmaxf, cfl_rate32(g, i, sig[q], uu[q], ww[q]));
+          }
+        }
+      }
+    }
+    __syncthreads();
+    finish_launch<kThreads32t>(ctl, si, (double)lmaxf, tid == 0 ? bsum : zsum, red);
+    return;
+  }
+
+  // ---- S0: every global load first (pairs, 8-byte aligned) ----
+  F2 ur[kItSrcP], wr[kItSrcP], sv[kItLoadP], pv[kItLoadP];
+#pragma unroll
+  for (int k = 0; k < kItSrcP; ++k) {
+    const int rs = wp + kWarps32p * k, i = ib + 1 + rs;
+    ur[k] = wr[k] = S(0.f);
+    if (rs < kSrcRows32t && row_ok(i)) {
+      const size_t q = (size_t)i * Nphi + jc;
+      ur[k] = *reinterpret_cast<const F2 *>(uu + q);
+      wr[k] = *reinterpret_cast<const F2 *>(ww + q);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kItLoadP; ++k) {
+    const int r = wp + kWarps32p * k, i = ib + r;
+    sv[k] = pv[k] = S(0.f);
+    if (r < kRows32t && row_ok(i)) {
+      const size_t q = (size_t)i * Nphi + jc;
+      sv[k] = *reinterpret_cast<const F2 *>(sig + q);
+      if (FM == kForcePhi) pv[k] = *reinterpret_cast<const F2 *>(Phi + q);
+    }
+  }
+  __syncthreads();  // row constants staged
+#pragma unroll
+  for (int k = 0; k < kItLoadP; ++k) {
+    const int r = wp + kWarps32p * k, i = ib + r;
+    if (r < kRows32t) {
+      const F2 s = sv[k];
+      F2 d = S(0.f);
+      if (row_ok(i)) {
+        if (G2) {
+          d = mul(mul(S(g.Kpoly), s), add(S(2.f * RC(tS0, i)), s));
+        } else {
+          const float P0 = RC(tP0, i), iS0 = RC(tInvS0, i);
+          d = make_float2(P0 * expm1f(g.gamma * log1pf(s.x * iS0)), P0 * expm1f(g.gamma * log1pf(s.y * iS0)));
+        }
+      }
+      SG[r * L2 + lane] = s;
+      DP[r * L2 + lane] = d;
+      PH[r * L2 + lane] = pv[k];
+    }
+  }
+  __syncthreads();
+
+  // ---- S2: source kick of rows i0-2 .. i0+kTileI+1 (hydro.hpp:73-96) ----
+#pragma unroll
+  for (int k = 0; k < kItSrcP; ++k) {
+    const int rs = wp + kWarps32p * k, r = rs + 1, i = ib + r;
+    if (rs < kSrcRows32t) {  // warp-uniform
+      const int x = r * L2 + lane;
+      const F2 dc = DP[x];
+      // azimuthal neighbours: column 2l-1 is the left lane's .y, 2l+2 the right lane's .x
+      const float dl = up1(dc.y), dr = dn1(dc.x);
+      F2 pc = S(0.f);
+      float pl = 0.f, pr = 0.f;
+      if (FM == kForcePhi) {
+        pc = PH[x];
+        pl = up1(pc.y);
+        pr = dn1(pc.x);
+      }
+      F2 nu1 = S(0.f), nw1 = S(0.f);
+      if (row_ok(i)) {
+        const F2 s_g = SG[x];
+        const F2 s = add(S(RC(tS0, i)), s_g);
+        const F2 pim = first_row(i) ? dc : DP[x - L2];
+        const F2 pip = last_row(i) ? dc : DP[x + L2];
+        const F2 ddP = mul(sub(pip, pim), S(RC(tInvdRc, i)));
+        const F2 dPdphi = mul(sub(make_float2(dc.y, dr), make_float2(dl, dc.x)), S(g.inv2dphi));
+        const float iR = RC(tInvR, i);
+        F2 dgR = S(0.f), dgp = S(0.f);
+        if (FM == kForcePhi) {
+          F2 dPhidu;
+          if (first_row(i)) dPhidu = mul(sub(PH[x + L2], pc), S(g.invdu));
+          else if (last_row(i)) dPhidu = mul(sub(pc, PH[x - L2]), S(g.invdu));
+          else dPhidu = mul(sub(PH[x + L2], PH[x - L2]), S(g.inv2du));
+          dgR = mul(dPhidu, S(-iR));
+          dgp = mul(mul(sub(make_float2(pc.y, pr), make_float2(pl, pc.x)), S(-g.inv2dphi)), S(iR));
+        } else if (FM == kForceArrays) {
+          const size_t q = (size_t)i * Nphi + jc;
+          dgR = make_float2((float)gRin[q], (float)gRin[q + 1]);
+          dgp = make_float2((float)gpin[q], (float)gpin[q + 1]);
+        }
+        const F2 uc = ur[k], wc = wr[k];
+        const float V = RC(tV0, i);
+        const F2 q1 = fdiv(sub(mul(mul(S(RC(tDP0, i)), s_g), S(RC(tInvS0, i))), ddP), s);
+        const F2 aR = add(add(add(S(RC(tA0, i)), q1), dgR), mul(mul(add(S(2.f * V), wc), wc), S(iR)));
+        const F2 q2 = fdiv(mul(dPdphi, S(-1.f)), mul(s, S(RC(tR, i))));
+        const F2 ap = sub(add(q2, dgp), mul(mul(uc, add(S(V), wc)), S(iR)));
+        nu1 = fma(S(dt), aR, uc);
+        nw1 = fma(S(dt), ap, wc);
+      }
+      U1[rs * L2 + lane] = nu1;
+      W1[rs * L2 + lane] = nw1;
+    }
+  }
+  __syncthreads();
+
+  // ---- S3: radial faces f = i0 .. i0+kTileI (hydro.hpp:107-130) ----
+#pragma unroll
+  for (int k = 0; k < kItFaceP; ++k) {
+    const int fr = wp + kWarps32p * k, f = i0 + fr;
+    if (fr < kFaceRows32t) {
+      F2 F = S(0.f), FRv = S(0.f), GAv = S(0.f), GBv = S(0.f);
+      if (IN || (f >= 1 && f <= Nu - 1)) {
+        const int xs = (f - 2 - ib) * L2 + lane;  // sigma rows f-2 .. f+1
+        const int xu = (f - 3 - ib) * L2 + lane;  // u1 / w1 rows f-2 .. f+1
+        const F2 s0 = SG[xs], s1 = SG[xs + L2], s2 = SG[xs + 2 * L2], s3 = SG[xs + 3 * L2];
+        const F2 u0 = U1[xu], u1 = U1[xu + L2], u2 = U1[xu + 2 * L2], u3 = U1[xu + 3 * L2];
+        const F2 w0 = W1[xu], w1 = W1[xu + L2], w2 = W1[xu + 2 * L2], w3 = W1[xu + 3 * L2];
+        const F2 vf = mul(S(0.5f), add(u1, u2));
+        const bool ux = vf.x > 0.f, uy = vf.y > 0.f;
+        const F2 vdt = mul(vf, S(dt));
+        const F2 hu = mul(S(0.5f), sub(S(1.f), mul(vdt, S(RC(tInvdRl, f)))));
+        const F2 hd = mul(S(-0.5f), add(S(1.f), mul(vdt, S(RC(tInvdRr, f)))));
+        const F2 hf = sel(ux, uy, hu, hd);
+        // cells cc-1, cc, cc+1 with cc = f-1 (upwind from below) or f
+        const F2 sa = sel(ux, uy, s0, s1), sb = sel(ux, uy, s1, s2), sc = sel(ux, uy, s2, s3);
+        const F2 ua = sel(ux, uy, u0, u1), ub = sel(ux, uy, u1, u2), uc = sel(ux, uy, u2, u3);
+        const F2 wa = sel(ux, uy, w0, w1), wb = sel(ux, uy, w1, w2), wc = sel(ux, uy, w2, w3);
+        const F2 ds_c = sels(ux, uy, RC(tDS0, f - 1), RC(tDS0, f)), ds_c1 = sels(ux, uy, RC(tDS0, f), RC(tDS0, f + 1));
+        const F2 dv_c = sels(ux, uy, RC(tDV, f - 1), RC(tDV, f)), dv_c1 = sels(ux, uy, RC(tDV, f), RC(tDV, f + 1));
+        const F2 s0_c = sels(ux, uy, RC(tS0, f - 1), RC(tS0, f));
+        F2 kS = vanleer(add(ds_c1, sub(sc, sb)), add(ds_c, sub(sb, sa)));
+        F2 kU = vanleer(sub(uc, ub), sub(ub, ua));
+        F2 kV = vanleer(add(dv_c1, sub(wc, wb)), add(dv_c, sub(wb, wa)));
+        if (!IN) {  // no slope in the first and last cell (hydro.hpp:117-119)
+          const int ccx = ux ? f - 1 : f, ccy = uy ? f - 1 : f;
+          const bool okx = ccx > 0 && ccx < Nu - 1, oky = ccy > 0 && ccy < Nu - 1;
+          kS = sel(okx, oky, kS, S(0.f));
+          kU = sel(okx, oky, kU, S(0.f));
+          kV = sel(okx, oky, kV, S(0.f));
+        }
+        const F2 Sf = fma(hf, kS, add(s0_c, sb));
+        const F2 uf = fma(hf, kU, ub);
+        const float dVf = RC(tDV, f);
+        const F2 Df = fma(hf, kV, add(sels(ux, uy, 0.f, dVf), wb));  // vphi_f - V0(f-1)
+        F = mul(mul(vf, Sf), S(RC(tAf, f)));
+        FRv = mul(F, uf);
+        GAv = mul(F, Df);
+        GBv = mul(F, sub(Df, S(dVf)));
+      }
+      const int x = fr * L2 + lane;
+      FF[x] = F; FR[x] = FRv; GA[x] = GAv; GB[x] = GBv;
+    }
+  }
+  __syncthreads();
+
+  // ---- S4: radial gather of rows i0 .. iend-1 (hydro.hpp:131-139), in place ----
+#pragma unroll
+  for (int k = 0; k < kItOutP; ++k) {
+    const int ri = wp + kWarps32p * k, i = i0 + ri;
+    if (IN || i < iend) {
+      const int xs = (i - ib) * L2 + lane, xu = (i - ib - 1) * L2 + lane, xf = ri * L2 + lane;
+      const F2 sgi = SG[xs], u1i = U1[xu], w1i = W1[xu];
+      const float S0 = RC(tS0, i), iv = RC(tInvVol, i);
+      const F2 s = add(S(S0), sgi);
+      const F2 s2 = fma(mul(S(dt), sub(FF[xf], FF[xf + L2])), S(iv), sgi);
+      const F2 sn = add(S(S0), s2);
+      const F2 d = make_float2(sn.x < 1e-10f ? 1e-10f : sn.x, sn.y < 1e-10f ? 1e-10f : sn.y);
+      const F2 u2 = fdiv(fma(mul(S(dt), sub(FR[xf], FR[xf + L2])), S(iv), mul(s, u1i)), d);
+      const F2 w2 = fdiv(fma(mul(S(dt), sub(GB[xf], GA[xf + L2])), S(iv), mul(s, w1i)), d);
+      SG[xs] = s2;
+      U2[xs] = u2;
+      W2[xs] = w2;
+    }
+  }
+  __syncthreads();
+
+  // ---- S5: azimuthal faces 2l and 2l+1 (left faces of those columns; hydro.hpp:150-170) ----
+#pragma unroll
+  for (int k = 0; k < kItOutP; ++k) {
+    const int ri = wp + kWarps32p * k, i = i0 + ri;
+    if (IN || i < iend) {
+      const int x = (i - ib) * L2 + lane;
+      const F2 sm = SG[x], um = U2[x], wm = W2[x];
+      // columns 2l-2, 2l-1 from the left lane, 2l+2 from the right lane
+      const float sL0 = up1(sm.x), sL1 = up1(sm.y), sR = dn1(sm.x);
+      const float uL0 = up1(um.x), uL1 = up1(um.y), uR = dn1(um.x);
+      const float wL0 = up1(wm.x), wL1 = up1(wm.y), wR = dn1(wm.x);
+      const float V = RC(tV0, i), idl = RC(tInvdl, i), S0 = RC(tS0, i), A = RC(tAphi, i);
+      const F2 dv = mul(S(0.5f), add(make_float2(wL1, wm.x), make_float2(wm.x, wm.y)));
+      const F2 vf = add(S(V), dv);
+      const bool ux = vf.x > 0.f, uy = vf.y > 0.f;
+      const F2 vdt = mul(mul(vf, S(dt)), S(idl));
+      const F2 hf = sel(ux, uy, mul(S(0.5f), sub(S(1.f), vdt)), mul(S(-0.5f), add(S(1.f), vdt)));
+      // face 2l: cells (2l-2, 2l-1, 2l) upwind from the left, else (2l-1, 2l, 2l+1);
+      // face 2l+1: (2l-1, 2l, 2l+1) or (2l, 2l+1, 2l+2)
+      const F2 sa = make_float2(ux ? sL0 : sL1, uy ? sL1 : sm.x), sb = make_float2(ux ? sL1 : sm.x, uy ? sm.x : sm.y),
+               sc = make_float2(ux ? sm.x : sm.y, uy ? sm.y : sR);
+      const F2 ua = make_float2(ux ? uL0 : uL1, uy ? uL1 : um.x), ub = make_float2(ux ? uL1 : um.x, uy ? um.x : um.y),
+               uc = make_float2(ux ? um.x : um.y, uy ? um.y : uR);
+      const F2 wa = make_float2(ux ? wL0 : wL1, uy ? wL1 : wm.x), wb = make_float2(ux ? wL1 : wm.x, uy ? wm.x : wm.y),
+               wc = make_float2(ux ? wm.x : wm.y, uy ? wm.y : wR);
+      const F2 sf = fma(hf, vanleer(sub(sc, sb), sub(sb, sa)), sb);
+      const F2 Sf = add(S(S0), sf);
+      const F2 uf = fma(hf, vanleer(sub(uc, ub), sub(ub, ua)), ub);
+      const F2 wf = fma(hf, vanleer(sub(wc, wb), sub(wb, wa)), wb);
+      const F2 Ffull = mul(mul(vf, Sf), S(A));
+      const int xf = ri * L2 + lane;
+      PF[xf] = mul(S(A), fma(S(V), sf, mul(dv, Sf)));
+      PR[xf] = mul(Ffull, uf);
+      PG[xf] = mul(Ffull, wf);
+    }
+  }
+  __syncthreads();
+
+  // ---- S6: azimuthal gather, floor (hydro.hpp:69), outputs, CFL rate ----
+#pragma unroll
+  for (int k = 0; k < kItOutP; ++k) {
+    const int ri = wp + kWarps32p * k, i = i0 + ri;
+    if (IN || i < iend) {
+      const int x = (i - ib) * L2 + lane, xf = ri * L2 + lane;
+      const F2 fm = PF[xf], fr = PR[xf], fg = PG[xf];
+      // right face of column 2l+1 is the right lane's first face
+      const F2 fm1 = make_float2(fm.y, dn1(fm.x)), fr1 = make_float2(fr.y, dn1(fr.x)), fg1 = make_float2(fg.y, dn1(fg.x));
+      if (outx || outy) {
+        const float iv = RC(tInvVol, i), S0 = RC(tS0, i);
+        const F2 s2 = SG[x], u2 = U2[x], w2 = W2[x];
+        const F2 sn2 = add(S(S0), s2);
+        F2 s3 = fma(mul(S(dt), sub(fm, fm1)), S(iv), s2);
+        const F2 sn3 = add(S(S0), s3);
+        const bool flx = sn3.x < 1e-10f, fly = sn3.y < 1e-10f;
+        const F2 d = make_float2(flx ? 1e-10f : sn3.x, fly ? 1e-10f : sn3.y);
+        const F2 u3 = fdiv(fma(mul(S(dt), sub(fr, fr1)), S(iv), mul(sn2, u2)), d);
+        const F2 w3 = fdiv(fma(mul(S(dt), sub(fg, fg1)), S(iv), mul(sn2, w2)), d);
+        s3 = make_float2(flx ? 1e-10f - S0 : s3.x, fly ? 1e-10f - S0 : s3.y);
+        const size_t q = (size_t)i * Nphi + jc;
+        const float R32 = RC(tR32, i);
+        const F2 xr = mul(S(R32), s3);
+        const __nv_bfloat16 hx = __float2bfloat16_rn(xr.x), hy = __float2bfloat16_rn(xr.y);
+        const __nv_bfloat16 lx = __float2bfloat16_rn(xr.x - __bfloat162float(hx));
+        const __nv_bfloat16 ly = __float2bfloat16_rn(xr.y - __bfloat162float(hy));
+        if (outx && outy) {
+          *reinterpret_cast<F2 *>(so + q) = s3;
+          *reinterpret_cast<F2 *>(uo + q) = u3;
+          *reinterpret_cast<F2 *>(wo + q) = w3;
+          *reinterpret_cast<__nv_bfloat162 *>(Sx.hi + q) = __halves2bfloat162(hx, hy);
+          *reinterpret_cast<__nv_bfloat162 *>(Sx.lo + q) = __halves2bfloat162(lx, ly);
+        } else {  // the last tile's edge: one element inside the grid
+          so[q] = s3.x; uo[q] = u3.x; wo[q] = w3.x;
+          Sx.hi[q] = hx;
+          Sx.lo[q] = lx;
+        }
+        // CFL rate of the new state (hydro.hpp:54-57)
+        const F2 scl = make_float2(flx ? 1e-10f : sn3.x, fly ? 1e-10f : sn3.y);
+        const float gk = g.gamma * g.Kpoly;
+        const F2 cs = G2 ? make_float2(sqrtf(gk * scl.x), sqrtf(gk * scl.y))
+                         : make_float2(sqrtf(gk * powf(scl.x, g.gamma - 1.f)), sqrtf(gk * powf(scl.y, g.gamma - 1.f)));
+        const float V = RC(tV0, i), idR = RC(tInvdR, i), idl = RC(tInvdl, i);
+        const F2 rate = fma(add(make_float2(fabsf(V + w3.x), fabsf(V + w3.y)), cs), S(idl),
+                            mul(add(make_float2(fabsf(u3.x), fabsf(u3.y)), cs), S(idR)));
+        if (outx) {
+          bad |= !(rate.x == rate.x) || !(u3.x == u3.x) || !(w3.x == w3.x);
+          lmaxf = fmaxf(lmaxf, rate.x);
+        }
+        if (outy) {
+          bad |= !(rate.y == rate.y) || !(u3.y == u3.y) || !(w3.y == w3.y);
+          lmaxf = fmaxf(lmaxf, rate.y);
+        }
+        S3[ri * L2 + lane] = s3;
+      }
+    }
+  }
+  // mode sums of the new state (output times and per-step diagnostics only)
+  if (si.nmodes) {
+    __syncthreads();
+    const double phx = (jc + 0.5) * (double)g.dphi, phy = (jc + 1.5) * (double)g.dphi;
+    for (int m = 0; m < si.nmodes; ++m) {
+      double re = 0.0, im = 0.0;
+      if (outx || outy) {
+        double snx, csx, sny, csy;
+        sincos(m * phx, &snx, &csx);
+        sincos(m * phy, &sny, &csy);
+#pragma unroll 1
+        for (int k = 0; k < kItOutP; ++k) {
+          const int ri = wp + kWarps32p * k, i = i0 + ri;
+          if (i < iend) {
+            const F2 s3 = S3[ri * L2 + lane];
+            const double dA = g.dAd[i], S0d = g.S0d[i];
+            if (outx) {
+              const double sf = S0d + (double)s3.x;
+              re += sf * csx * dA;
+              im -= sf * snx * dA;
+            }
+            if (outy) {
+              const double sf = S0d + (double)s3.y;
+              re += sf * csy * dA;
+              im -= sf * sny * dA;
+            }
+          }
+        }
+      }
+      re = warp_sum(re);
+      im = warp_sum(im);
+      if (lane == 0) {
+        atomicAdd(&bsum[2 * m], re);
+        atomicAdd(&bsum[2 * m + 1], im);
+      }
+    }
+  }
+  __syncthreads();
+  double lmax = (double)lmaxf;
+  if (bad) lmax = __longlong_as_double(0x7ff8000000000000ll);
+  finish_launch<kThreads32t>(ctl, si, lmax, tid == 0 ? bsum : zsum, red);
+#undef RC
+}
+
+template <bool G2, int FM>
+__global__ void __launch_bounds__(kThreads32t, 3) k_hydro32p(
+    const float *__restrict__ sig, const float *__restrict__ uu, const float *__restrict__ ww,
+    const float *__restrict__ Phi, const double *__restrict__ gRin, const double *__restrict__ gpin,
+    float *__restrict__ so, float *__restrict__ uo, float *__restrict__ wo, SplitBf16 Sx, Ctl *ctl, Rows32 g) {
+  extern __shared__ float sm32t[];
+  __shared__ double red[kThreads32t / 32];
+  __shared__ double bsum[2 * kMaxModes], zsum[2 * kMaxModes];
+  const int i0 = blockIdx.y * kTileI;
+  if (i0 >= 3 && i0 + kTileI + 3 <= g.Nu)
+    hydro32p_tile<G2, FM, true>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum);
+  else
+    hydro32p_tile<G2, FM, false>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum);
+}
+
+}  // namespace dg

@@ -16,6 +16,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
 #include <utility>
 #include <vector>
 
@@ -27,6 +30,7 @@
 #include "step_ctl.cuh"
 #include "hydro32w.cuh"
 #include "hydro32t.cuh"
+#include "hydro32p.cuh"
 #include "uconv.cuh"
 
 using namespace dg;
@@ -58,9 +62,16 @@ struct MixedState {
   SplitBuf Xin, Tb, Yk, Ub, RB, RA, RGA, RGB;
   float *KW2 = nullptr;
   float2 *tw = nullptr;
-  // hydro kernel: the tiled form (hydro32t.cuh) unless DISKGPU_HYDRO32=warp selects the
-  // warp-marching form (hydro32w.cuh); both compute the same step
-  bool hydro_tile = true;
+  // hydro kernel: the tiled form (hydro32t.cuh), its packed two-column form (hydro32p.cuh)
+  // or the warp-marching form (hydro32w.cuh), chosen by DISKGPU_HYDRO32 = tile | packed |
+  // warp; all compute the same step
+  enum HydroKind : int { kHydroWarp = 0, kHydroTile = 1, kHydroPacked = 2 };
+  int hydro_kind = kHydroTile;
+  // pipeline stages of each gravity product (slots: 0 phi DFT, 1-4 the u passes, 5 inverse
+  // phi DFT; 0 = chosen by K) and the tuner's record (autotune below)
+  int ns[6] = {0, 0, 0, 0, 0, 0};
+  bool tuned = false;
+  std::string tune_info;
   // A = 32 (Nu = 1024): the four u passes run as one fused kernel (uconv.cuh)
   bool fused_u = false;
   float *khm = nullptr;  // khat[m][p] / M, [nm][M]
@@ -85,11 +96,14 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // K-major BF16 matrix [rows][cols] -> tiles of box_rows x 64 with 128-byte swizzle.
-// every instantiation of the tiled hydro kernel takes more than 48 KB of shared memory
+// every instantiation of the tiled hydro kernels takes more than 48 KB of shared memory
 static cudaError_t hydro32t_prepare() {
   const void *fns[] = {(const void *)k_hydro32t<true, kForcePhi>, (const void *)k_hydro32t<false, kForcePhi>,
                        (const void *)k_hydro32t<true, kForceArrays>, (const void *)k_hydro32t<false, kForceArrays>,
-                       (const void *)k_hydro32t<true, kForceNone>, (const void *)k_hydro32t<false, kForceNone>};
+                       (const void *)k_hydro32t<true, kForceNone>, (const void *)k_hydro32t<false, kForceNone>,
+                       (const void *)k_hydro32p<true, kForcePhi>, (const void *)k_hydro32p<false, kForcePhi>,
+                       (const void *)k_hydro32p<true, kForceArrays>, (const void *)k_hydro32p<false, kForceArrays>,
+                       (const void *)k_hydro32p<true, kForceNone>, (const void *)k_hydro32p<false, kForceNone>};
   for (const void *f : fns) {
     cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem32t);
     if (e != cudaSuccess) return e;
@@ -436,9 +450,10 @@ static cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, siz
   return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
+// gemm(): one split-BF16 product.  ns = pipeline stages (1, 2 or 4); 0 picks by K.
 template <int MODE, bool A_MN = false, bool B_MN = false>
 static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUtensorMap &Bh, const CUtensorMap &Bl,
-                        int M, int N, int K, const tc::GemmArgs &base, cudaStream_t st) {
+                        int M, int N, int K, const tc::GemmArgs &base, cudaStream_t st, int ns = 0) {
   tc::GemmArgs a = base;
   a.M = M; a.N = N; a.K = K;
   if (M % tc::BM || N % tc::BN || K % tc::BK) return cudaErrorInvalidValue;
@@ -446,10 +461,11 @@ static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUte
   // short contractions (one or two K chunks) need no deep pipeline: fewer stages let more
   // CTAs share an SM and hide each tile's load / epilogue latency
   const int nk = K / tc::BK;
-  if (nk <= 1)
+  if (ns == 0) ns = nk <= 1 ? 1 : (nk <= 2 ? 2 : tc::STAGES);
+  if (ns <= 1)
     return launch_pdl(tc::k_gemm_split<MODE, A_MN, B_MN, 1>, grid, dim3(tc::kThreads), tc::smem_bytes(1), st, Ah, Al,
                       Bh, Bl, a);
-  if (nk <= 2)
+  if (ns <= 2)
     return launch_pdl(tc::k_gemm_split<MODE, A_MN, B_MN, 2>, grid, dim3(tc::kThreads), tc::smem_bytes(2), st, Ah, Al,
                       Bh, Bl, a);
   return launch_pdl(tc::k_gemm_split<MODE, A_MN, B_MN, tc::STAGES>, grid, dim3(tc::kThreads),
@@ -570,8 +586,11 @@ int dg_handle::mixed_init() {
   XK(cudaStreamSynchronize(st));
   {
     const char *hk = getenv("DISKGPU_HYDRO32");
-    X.hydro_tile = !(hk && strcmp(hk, "warp") == 0) && Nphi >= kLd32t;
-    if (X.hydro_tile) XK(hydro32t_prepare());
+    X.hydro_kind = MixedState::kHydroTile;
+    if (hk && strcmp(hk, "warp") == 0) X.hydro_kind = MixedState::kHydroWarp;
+    if (hk && strcmp(hk, "packed") == 0) X.hydro_kind = MixedState::kHydroPacked;
+    if (Nphi < kLd32t || Nphi % 2) X.hydro_kind = MixedState::kHydroWarp;
+    if (X.hydro_kind != MixedState::kHydroWarp) XK(hydro32t_prepare());
   }
   X.tables_ready = true;
   return DG_OK;
@@ -714,6 +733,10 @@ static int build_basic(dg_handle *h, const double *Sig, const double *vp) {
   return DG_OK;
 }
 
+static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *u, const float *w, const float *Phi,
+                                  const double *gR, const double *gp, int fm, float *so, float *uo, float *wo, Ctl *ctl,
+                                  cudaStream_t st);
+
 int dg_handle::mixed_upload_state(const double *Sig, const double *vRh, const double *vph) {
   MixedState &X = *mx;
   const size_t n = (size_t)p.Nu * p.Nphi;
@@ -727,8 +750,178 @@ int dg_handle::mixed_upload_state(const double *Sig, const double *vRh, const do
   XK(cudaMemcpyAsync(VP[0], vph, n * sizeof(double), cudaMemcpyHostToDevice, st));
   k_to_pert<<<grid_for(n), 256, 0, st>>>(S[0], VR[0], VP[0], X.sig[cur], X.u[cur], X.w[cur], X.Sx, X.rows);
   XK(cudaGetLastError());
+  if (!in_step_host && !X.tuned) {
+    int rc = mixed_autotune();
+    if (rc) return rc;
+    // the tuning launches overwrote the gravity operand: rebuild it from the uploaded state
+    k_to_pert<<<grid_for(n), 256, 0, st>>>(S[0], VR[0], VP[0], X.sig[cur], X.u[cur], X.w[cur], X.Sx, X.rows);
+    XK(cudaGetLastError());
+  }
   return DG_OK;
 }
+
+// ---------------------------------------------------------------------------------
+// Autotuner.  At a handle's first state upload (dg_set_state, dg_init_standard, dg_load;
+// never inside a stream capture) it times the step's kernel variants on the handle's own
+// buffers and keeps the fastest:
+//   * the pipeline depth (1, 2 or 4 stages) of every gravity product, one product at a time
+//     with the others fixed, timing the whole gravity of the uploaded state;
+//   * the hydro form (tiled, packed two-column, warp-marching), writing the other ping-pong
+//     buffers and a scratch control block, so the handle's dt, time and records are untouched.
+// A variant must beat the current choice by 2 % to replace it.  Choices are cached per
+// process by (Nu, Nphi, Gamma = 2, self-gravity), so the disks of a batch that share a grid
+// are tuned once.  DISKGPU_TUNE=0 keeps the defaults (tiled hydro, stages by K);
+// DISKGPU_HYDRO32 fixes the hydro form.
+namespace {
+struct TuneKey {
+  int Nu, Nphi, g2, sg;
+  bool operator<(const TuneKey &o) const {
+    if (Nu != o.Nu) return Nu < o.Nu;
+    if (Nphi != o.Nphi) return Nphi < o.Nphi;
+    if (g2 != o.g2) return g2 < o.g2;
+    return sg < o.sg;
+  }
+};
+struct TuneVal {
+  int hydro_kind;
+  int ns[6];
+  std::string info;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune_cache;
+const char *kHydroNames[3] = {"warp", "tile", "packed"};
+}  // namespace
+
+int dg_handle::mixed_autotune() {
+  MixedState &X = *mx;
+  X.tuned = true;
+  const char *env = getenv("DISKGPU_TUNE");
+  if (env && strcmp(env, "0") == 0) {
+    X.tune_info = "tuning off: hydro " + std::string(kHydroNames[X.hydro_kind]) + ", stages by K";
+    return DG_OK;
+  }
+  const char *hk = getenv("DISKGPU_HYDRO32");
+  // the warp form is the only one for odd or narrow grids; a user's choice stands
+  const bool hydro_fixed = (hk && *hk) || X.hydro_kind == MixedState::kHydroWarp;
+  const TuneKey key{p.Nu, p.Nphi, X.rows.gamma2, p.selfgrav};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      if (!hydro_fixed) X.hydro_kind = it->second.hydro_kind;
+      memcpy(X.ns, it->second.ns, sizeof(X.ns));
+      X.tune_info = it->second.info + " (cached)";
+      return DG_OK;
+    }
+  }
+  const bool prof_was = prof_on;
+  prof_on = false;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  XK(cudaEventCreate(&e0));
+  XK(cudaEventCreate(&e1));
+  Ctl *sctl = nullptr;
+  int rc = DG_OK;
+  char buf[256];
+  std::string info;
+  // best of 3 timed runs after one warm-up, in microseconds
+  auto time_us = [&](auto &&fn, float *best) -> cudaError_t {
+    *best = 1e30f;
+    for (int r = 0; r < 4; ++r) {
+      cudaError_t e = fn(true);
+      if (e != cudaSuccess) return e;
+      if ((e = cudaEventRecord(e0, st)) != cudaSuccess) return e;
+      if ((e = fn(false)) != cudaSuccess) return e;
+      if ((e = cudaEventRecord(e1, st)) != cudaSuccess) return e;
+      if ((e = cudaEventSynchronize(e1)) != cudaSuccess) return e;
+      float ms = 0.f;
+      if ((e = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) return e;
+      if (r > 0 && 1e3f * ms < *best) *best = 1e3f * ms;
+    }
+    return cudaSuccess;
+  };
+  do {
+    if (p.selfgrav) {
+      const std::vector<int> slots = !X.factored ? std::vector<int>{0, 1, 2, 5}
+                                     : (X.fused_u ? std::vector<int>{0, 5} : std::vector<int>{0, 1, 2, 3, 4, 5});
+      auto grav = [&](bool) -> cudaError_t { return mixed_gravity() ? cudaErrorUnknown : cudaSuccess; };
+      float tbest;
+      cudaError_t e = time_us(grav, &tbest);
+      if (e != cudaSuccess) { rc = fail(DG_ERR_CUDA, "autotune", cudaGetErrorString(e)); break; }
+      const float t0 = tbest;
+      for (int sl : slots) {
+        int keep = X.ns[sl];
+        for (int cand : {1, 2, 4}) {
+          X.ns[sl] = cand;
+          float t;
+          if ((e = time_us(grav, &t)) != cudaSuccess) break;
+          if (t < 0.98f * tbest) {
+            tbest = t;
+            keep = cand;
+          }
+        }
+        X.ns[sl] = keep;
+        if (e != cudaSuccess) break;
+      }
+      if (e != cudaSuccess) { rc = fail(DG_ERR_CUDA, "autotune", cudaGetErrorString(e)); break; }
+      snprintf(buf, sizeof buf, "gravity %.1f us (stages by K: %.1f us), stages", tbest, t0);
+      info += buf;
+      for (int sl : slots) {
+        snprintf(buf, sizeof buf, " %d", X.ns[sl] ? X.ns[sl] : 0);
+        info += buf;
+      }
+    }
+    if (!hydro_fixed) {
+      if (cudaMalloc(&sctl, sizeof(Ctl)) != cudaSuccess) { rc = fail(DG_ERR_NOMEM, "autotune", "control block"); break; }
+      Ctl h0;
+      memset(&h0, 0, sizeof h0);
+      h0.t = 0.0; h0.tlim = 1e300; h0.cfl = 0.3; h0.dt = 1e-7; h0.tnext = 1e300; h0.dtout = 1.0; h0.mD = 1.0;
+      h0.fixed_dt = 1;
+      const int fm = p.selfgrav ? kForcePhi : kForceNone;
+      const int c = cur, o = cur ^ 1;
+      auto hyd = [&](bool) -> cudaError_t {
+        cudaError_t e = cudaMemcpyAsync(sctl, &h0, sizeof(Ctl), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+        return launch_hydro32(X, X.sig[c], X.u[c], X.w[c], X.dPhi, nullptr, nullptr, fm, X.sig[o], X.u[o], X.w[o],
+                              sctl, st);
+      };
+      const int kinds[3] = {MixedState::kHydroTile, MixedState::kHydroPacked, MixedState::kHydroWarp};
+      float tk[3] = {0.f, 0.f, 0.f};
+      int best = MixedState::kHydroTile;
+      float tb = 1e30f;
+      cudaError_t e = cudaSuccess;
+      for (int q = 0; q < 3 && e == cudaSuccess; ++q) {
+        X.hydro_kind = kinds[q];
+        e = time_us(hyd, &tk[q]);
+        if (e == cudaSuccess && (q == 0 || tk[q] < 0.98f * tb)) {
+          tb = tk[q];
+          best = kinds[q];
+        }
+      }
+      X.hydro_kind = best;
+      if (e != cudaSuccess) { rc = fail(DG_ERR_CUDA, "autotune", cudaGetErrorString(e)); break; }
+      snprintf(buf, sizeof buf, "%shydro %s (tile %.1f us, packed %.1f us, warp %.1f us)", info.empty() ? "" : "; ",
+               kHydroNames[best], tk[0], tk[1], tk[2]);
+      info += buf;
+    } else {
+      info += std::string(info.empty() ? "" : "; ") + "hydro " + kHydroNames[X.hydro_kind] + " (fixed)";
+    }
+  } while (false);
+  if (sctl) cudaFree(sctl);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  prof_on = prof_was;
+  if (rc) return rc;
+  X.tune_info = info;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  TuneVal v;
+  v.hydro_kind = X.hydro_kind;
+  memcpy(v.ns, X.ns, sizeof(v.ns));
+  v.info = info;
+  g_tune_cache[key] = v;
+  return DG_OK;
+}
+
+std::string dg_handle::mixed_tuning_info() const { return mx ? mx->tune_info : std::string(); }
 
 int dg_handle::mixed_download_state(double *Sig, double *vRh, double *vph) {
   MixedState &X = *mx;
@@ -745,7 +938,20 @@ int dg_handle::mixed_download_state(double *Sig, double *vRh, double *vph) {
 static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *u, const float *w, const float *Phi,
                                   const double *gR, const double *gp, int fm, float *so, float *uo, float *wo, Ctl *ctl,
                                   cudaStream_t st) {
-  if (X.hydro_tile) {
+  if (X.hydro_kind == MixedState::kHydroPacked) {
+    dim3 grid((X.Nphi + kTileJp - 1) / kTileJp, (X.Nu + kTileI - 1) / kTileI);
+    const SplitBf16 sx{X.Sx.hi, X.Sx.lo};
+    cudaError_t e = cudaSuccess;
+    auto go = [&](auto kern) {
+      e = launch_pdl(kern, grid, dim3(kThreads32t), kSmem32t, st, sig, u, w, Phi, gR, gp, so, uo, wo, sx, ctl, X.rows);
+    };
+    const bool g2 = X.rows.gamma2 != 0;
+    if (fm == kForcePhi) g2 ? go(k_hydro32p<true, kForcePhi>) : go(k_hydro32p<false, kForcePhi>);
+    else if (fm == kForceArrays) g2 ? go(k_hydro32p<true, kForceArrays>) : go(k_hydro32p<false, kForceArrays>);
+    else g2 ? go(k_hydro32p<true, kForceNone>) : go(k_hydro32p<false, kForceNone>);
+    return e;
+  }
+  if (X.hydro_kind == MixedState::kHydroTile) {
     dim3 grid((X.Nphi + kTileJ - 1) / kTileJ, (X.Nu + kTileI - 1) / kTileI);
     const SplitBf16 sx{X.Sx.hi, X.Sx.lo};
     cudaError_t e = cudaSuccess;
@@ -778,7 +984,7 @@ int dg_handle::mixed_gravity() {
     // G1: phi DFT, stored as the F1 operand Xin[(i2, ri)][(m, i1)]
     a.out_hi = X.Xin.hi; a.out_lo = X.Xin.lo;
     XK(prof_begin(DG_PROF_GRAV_PHI_FWD));
-    XK(gemm<tc::kEpiPhiToXin>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st));
+    XK(gemm<tc::kEpiPhiToXin>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st, X.ns[0]));
     XK(prof_end(DG_PROF_GRAV_PHI_FWD));
     XK(prof_begin(DG_PROF_GRAV_U));
     if (X.fused_u) {
@@ -789,42 +995,45 @@ int dg_handle::mixed_gravity() {
     } else {
       // F1: 64-point DFT over i2 (K = 32 complex), twiddle, -> Tb[(i1, ri)][(m, p2)]
       a.out_hi = X.Tb.hi; a.out_lo = X.Tb.lo;
-      XK((gemm<tc::kEpiTwiddleF1, false, true>(X.mRB[0], X.mRB[1], X.mXin[0], X.mXin[1], 128, nm * A, 64, a, st)));
+      XK((gemm<tc::kEpiTwiddleF1, false, true>(X.mRB[0], X.mRB[1], X.mXin[0], X.mXin[1], 128, nm * A, 64, a, st,
+                                                 X.ns[1])));
       // F2: A-point DFT over i1, x khat / M -> Yk[(m, p2)][(p1, ri)]
       a.out_hi = X.Yk.hi; a.out_lo = X.Yk.lo; a.ldo = 2 * A; a.table = X.KW2;
-      XK((gemm<tc::kEpiSplitScaled, true, false>(X.mTb[0], X.mTb[1], X.mRA[0], X.mRA[1], nm * 64, 2 * A, 2 * A, a, st)));
+      XK((gemm<tc::kEpiSplitScaled, true, false>(X.mTb[0], X.mTb[1], X.mRA[0], X.mRA[1], nm * 64, 2 * A, 2 * A, a,
+                                                   st, X.ns[2])));
       // I1: inverse A-point DFT over p1, conjugate twiddle -> Ub[(m, i1)][(p2, ri)]
       a.out_hi = X.Ub.hi; a.out_lo = X.Ub.lo; a.table = nullptr;
-      XK(gemm<tc::kEpiTwiddleI1>(X.mYk[0], X.mYk[1], X.mRGA[0], X.mRGA[1], nm * 64, 2 * A, 2 * A, a, st));
+      XK(gemm<tc::kEpiTwiddleI1>(X.mYk[0], X.mYk[1], X.mRGA[0], X.mRGA[1], nm * 64, 2 * A, 2 * A, a, st, X.ns[3]));
       // I2: inverse 64-point DFT over p2 (the 32 physical i2) -> Z[c][i]
       a.out_hi = X.Z.hi; a.out_lo = X.Z.lo;
-      XK(gemm<tc::kEpiI2ToZ>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st));
+      XK(gemm<tc::kEpiI2ToZ>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st, X.ns[4]));
     }
     XK(prof_end(DG_PROF_GRAV_U));
     // G4: inverse phi DFT with Z as an MN-major operand
     a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi; a.row_scale = X.phiscale;
     XK(prof_begin(DG_PROF_GRAV_PHI_INV));
-    XK((gemm<tc::kEpiRowScaleF32, true, false>(X.mZmn[0], X.mZmn[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st)));
+    XK((gemm<tc::kEpiRowScaleF32, true, false>(X.mZmn[0], X.mZmn[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st,
+                                               X.ns[5])));
     XK(prof_end(DG_PROF_GRAV_PHI_INV));
     return DG_OK;
   }
   // G1: X1[c][i] = Fphi[c][:] . Sx[i][:]
   a.out_hi = X.X1.hi; a.out_lo = X.X1.lo; a.ldo = Nu;
   XK(prof_begin(DG_PROF_GRAV_PHI_FWD));
-  XK(gemm<tc::kEpiSplit>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st));
+  XK(gemm<tc::kEpiSplit>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st, X.ns[0]));
   XK(prof_end(DG_PROF_GRAV_PHI_FWD));
   // G2: Wt[c][p] = KW[c][p] * X1[c][:] . Cu[p][:]
   a.out_hi = X.Wt.hi; a.out_lo = X.Wt.lo; a.ldo = 2 * Nu; a.table = X.KW;
   XK(prof_begin(DG_PROF_GRAV_U));
-  XK(gemm<tc::kEpiSplitScaled>(X.mX1[0], X.mX1[1], X.mCu[0], X.mCu[1], Nphi, 2 * Nu, Nu, a, st));
+  XK(gemm<tc::kEpiSplitScaled>(X.mX1[0], X.mX1[1], X.mCu[0], X.mCu[1], Nphi, 2 * Nu, Nu, a, st, X.ns[1]));
   // G3: Z[i][c] = CuT[i][:] . Wt[c][:]
   a.out_hi = X.Z.hi; a.out_lo = X.Z.lo; a.ldo = Nphi; a.table = nullptr;
-  XK(gemm<tc::kEpiSplit>(X.mCuT[0], X.mCuT[1], X.mWt[0], X.mWt[1], Nu, Nphi, 2 * Nu, a, st));
+  XK(gemm<tc::kEpiSplit>(X.mCuT[0], X.mCuT[1], X.mWt[0], X.mWt[1], Nu, Nphi, 2 * Nu, a, st, X.ns[2]));
   XK(prof_end(DG_PROF_GRAV_U));
   // G4: dPhi[i][j] = phiscale[i] * Z[i][:] . Gphi[j][:]
   a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi; a.row_scale = X.phiscale;
   XK(prof_begin(DG_PROF_GRAV_PHI_INV));
-  XK(gemm<tc::kEpiRowScaleF32>(X.mZ[0], X.mZ[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st));
+  XK(gemm<tc::kEpiRowScaleF32>(X.mZ[0], X.mZ[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st, X.ns[5]));
   XK(prof_end(DG_PROF_GRAV_PHI_INV));
   return DG_OK;
 }

@@ -57,7 +57,7 @@ EXPORTS = (
     "dg_params_default", "dg_create", "dg_destroy", "dg_last_error", "dg_status_string", "dg_grid",
     "dg_init_standard", "dg_set_state", "dg_get_state", "dg_timestep", "dg_step", "dg_step_forces",
     "dg_potential", "dg_forces", "dg_disk_mass", "dg_modes", "dg_conserved", "dg_advance", "dg_time",
-    "dg_set_stream", "dg_run_steps", "dg_step_host", "dg_profile_enable", "dg_profile_read", "dg_kernels_per_step",
+    "dg_set_stream", "dg_run_steps", "dg_step_host", "dg_profile_enable", "dg_profile_read", "dg_kernels_per_step", "dg_tuning_info",
     "dg_timestep_static", "dg_rotation_curve_elliptic", "dg_params_physical",
     "dg_batch_create", "dg_batch_destroy", "dg_batch_last_error", "dg_batch_size", "dg_batch_disk",
     "dg_batch_init_standard", "dg_batch_advance", "dg_save", "dg_load", "dg_set_diagnostics",
@@ -113,6 +113,7 @@ def lib():
     L.dg_profile_enable.argtypes = [H, C.c_int]
     L.dg_profile_read.argtypes = [H, D, C.POINTER(C.c_longlong)]
     L.dg_kernels_per_step.argtypes = [H]
+    L.dg_tuning_info.argtypes = [H, C.c_char_p, C.c_int]
     L.dg_rotation_curve_elliptic.argtypes = [C.POINTER(Params), C.c_int, D, D, D, D, D]
     L.dg_params_physical.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(Params), D]
     L.dg_batch_create.argtypes = [C.c_int, C.POINTER(Params), C.POINTER(H)]
@@ -369,6 +370,12 @@ class Disk:
         cnt = (C.c_longlong * PROF_N)()
         self._ck(lib().dg_profile_read(self.h, _dp(ms), cnt))
         return {PROF_NAMES[k]: (float(ms[k]), int(cnt[k])) for k in range(PROF_N)}
+
+    def tuning(self):
+        """The autotuner's choices for this disk (one line of text)."""
+        buf = C.create_string_buffer(512)
+        self._ck(lib().dg_tuning_info(self.h, buf, 512))
+        return buf.value.decode()
 
     def kernels_per_step(self):
         """How many of this library's kernels one time step launches."""

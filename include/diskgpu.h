@@ -235,6 +235,12 @@ int dg_profile_read(dg_handle *h, double *ms, long long *count);
 /* Number of this library's kernels one time step of the handle launches (gravity passes
  * plus the fused hydro kernel); depends on precision, grid and self-gravity. */
 int dg_kernels_per_step(const dg_handle *h);
+/* What the autotuner chose for this handle, as one line of text (NUL-terminated, cut to
+ * len bytes): the hydro kernel form and the pipeline depth of each gravity product, with
+ * the timings behind the choice.  No counterpart in the reference.  The tuner runs at the
+ * first dg_set_state / dg_init_standard / dg_load of a mixed-precision handle and caches its
+ * choices per process by grid; DISKGPU_TUNE=0 in the environment keeps the defaults. */
+int dg_tuning_info(const dg_handle *h, char *buf, int len);
 
 /* Allocation-free CFL time step.  No counterpart in the reference: it is the same
  * dt = cfl / max_ij (sR + sphi) as dg_timestep, for callers that may not allocate device

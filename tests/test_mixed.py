@@ -108,19 +108,19 @@ def test_mixed_nonfinite_reported():
         assert e.value.code == -3
 
 
-@pytest.mark.parametrize("N,steps,rec", [(256, 40, False), (1024, 12, False), (128, 30, True)])
-def test_tiled_hydro_matches_warp_form(N, steps, rec, monkeypatch):
-    """The tiled hydro kernel (default) and the warp-marching kernel (DISKGPU_HYDRO32=warp)
-    compute the same step with the same expressions; they differ only in how the compiler
-    contracts them into FMAs, which the near-cancellation of the radial force amplifies.
-    States agree to <= 1e-4 of the perturbation's size after the given steps (an indexing
-    or halo error shows up at O(1)), dt and mode records to 1e-6."""
+@pytest.mark.parametrize("form", ["tile", "packed"])
+@pytest.mark.parametrize("N,steps,rec", [(256, 40, False), (1024, 12, False), (128, 30, True), (384, 20, False)])
+def test_tiled_hydro_matches_warp_form(N, steps, rec, form, monkeypatch):
+    """The tiled hydro kernel, its packed two-column form (DISKGPU_HYDRO32=tile / packed)
+    and the warp-marching kernel (DISKGPU_HYDRO32=warp) compute the same step with the same
+    expressions; they differ only in how the compiler contracts them into FMAs, which the
+    near-cancellation of the radial force amplifies.  States agree to <= 1e-4 of the
+    perturbation's size after the given steps (an indexing or halo error shows up at O(1)),
+    dt and mode records to 1e-6.  384 is not a multiple of either tile width, so the last
+    column of tiles is partial."""
     out = []
-    for form in ("tile", "warp"):
-        if form == "warp":
-            monkeypatch.setenv("DISKGPU_HYDRO32", "warp")
-        else:
-            monkeypatch.delenv("DISKGPU_HYDRO32", raising=False)
+    for kind in (form, "warp"):
+        monkeypatch.setenv("DISKGPU_HYDRO32", kind)
         with D.Disk(N, N, eps=0.005, amp=1e-2, precision="mixed") as d:
             d.init_standard()
             S0 = d.get_state()[0].mean(axis=1, keepdims=True)
@@ -142,3 +142,25 @@ def test_tiled_hydro_matches_warp_form(N, steps, rec, monkeypatch):
     if rec:
         assert len(ra) == len(rb) and len(ra) >= 3
         np.testing.assert_allclose(ra[:, 1:3], rb[:, 1:3], rtol=1e-6)
+
+
+def test_autotuner_reports_its_choice(monkeypatch):
+    """The autotuner runs at the first state upload, leaves the state and dt untouched, and
+    says what it chose; DISKGPU_TUNE=0 keeps the defaults; a second disk of the same grid
+    reuses the cached choice."""
+    monkeypatch.delenv("DISKGPU_HYDRO32", raising=False)
+    with D.Disk(256, 512, eps=0.005, amp=1e-3, precision="mixed") as a:
+        a.init_standard()
+        info = a.tuning()
+        assert "hydro" in info and "gravity" in info and "cached" not in info
+        dt_tuned = a.timestep(0.3)
+        S_tuned = a.get_state()[0]
+    with D.Disk(256, 512, eps=0.005, amp=1e-3, precision="mixed") as b:
+        b.init_standard()
+        assert b.tuning().endswith("(cached)")
+    monkeypatch.setenv("DISKGPU_TUNE", "0")
+    with D.Disk(256, 512, eps=0.005, amp=1e-3, precision="mixed") as c:
+        c.init_standard()
+        assert c.tuning().startswith("tuning off")
+        assert c.timestep(0.3) == dt_tuned
+        np.testing.assert_array_equal(c.get_state()[0], S_tuned)
