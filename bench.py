@@ -228,6 +228,10 @@ def gravity_parts(precision, Nu, Nphi):
                 ("grav_phi_inv", "FP64 smem FFT, phi inverse + scaling (k_phi_inv)", "hbm", spec + 8 * Nu * Nphi, "B")]
     # split-BF16 tcgen05 products: 3 MMAs per term, 2 flops per MAC
     g1 = 6 * Nphi * Nu * Nphi
+    g1name = "phi DFT GEMM (k_gemm_split, split-BF16)"
+    if Nu == 1024 and Nphi == 1024:  # fused two-stage transform: 4 rows per CTA, 2 products
+        g1 = (Nu // 4) * (6 * 128 * 128 * 32 + 6 * 128 * 64 * 64)
+        g1name = "fused phi transform (k_phifwd: real 32-point + complex 32-point tcgen05 stages)"
     g4 = 6 * Nu * Nphi * Nphi
     if Nu % 1024 == 0:
         A, nm = Nu // 32, ((Nphi // 2 + 1) + 3) // 4 * 4
@@ -237,7 +241,7 @@ def gravity_parts(precision, Nu, Nphi):
     else:
         u = 6 * Nphi * 2 * Nu * Nu + 6 * Nu * Nphi * 2 * Nu
         uname = "dense u DFT x khat (two k_gemm_split passes)"
-    return [("grav_phi_fwd", "phi DFT GEMM (k_gemm_split, split-BF16)", "tensor", g1, "flop"),
+    return [("grav_phi_fwd", g1name, "tensor", g1, "flop"),
             ("grav_u", uname, "tensor", u, "flop"),
             ("grav_phi_inv", "inverse phi DFT GEMM + potential scaling (k_gemm_split)", "tensor", g4, "flop")]
 

@@ -32,6 +32,7 @@
 #include "hydro32t.cuh"
 #include "hydro32p.cuh"
 #include "uconv.cuh"
+#include "phifwd.cuh"
 
 using namespace dg;
 
@@ -75,6 +76,11 @@ struct MixedState {
   // A = 32 (Nu = 1024): the four u passes run as one fused kernel (uconv.cuh)
   bool fused_u = false;
   float *khm = nullptr;  // khat[m][p] / M, [nm][M]
+  // Nu = Nphi = 1024: the forward phi transform as one fused kernel (phifwd.cuh)
+  bool fused_phi = false;
+  SplitBuf PA, PB;       // its stage-A (real 32-point) and stage-B (complex 32-point) operands
+  float2 *twphi = nullptr;  // W^{m2 j1}, [32][32]
+  CUtensorMap mPA[2], mPB[2];
   float2 *twp = nullptr; // W_M^{p2 i1} with padded rows, [64][kUcTwLd]
   CUtensorMap mXin[2], mTb[2], mYk[2], mUb[2], mRB[2], mRA[2], mRGA[2], mRGB[2], mZmn[2];
   bool tables_ready = false;
@@ -95,7 +101,15 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// K-major BF16 matrix [rows][cols] -> tiles of box_rows x 64 with 128-byte swizzle.
+// Dynamic shared memory of a step kernel, and the largest shared-memory carveout for all of
+// them: the step's kernels alternate between 1 and 4 CTAs per SM with 46 to 214 KB each, and
+// one common L1 / shared split spares the SMs a reconfiguration at every kernel boundary.
+static cudaError_t smem_attrs(const void *fn, size_t bytes) {
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+}
+
 // every instantiation of the tiled hydro kernels takes more than 48 KB of shared memory
 static cudaError_t hydro32t_prepare() {
   const void *fns[] = {(const void *)k_hydro32t<true, kForcePhi>, (const void *)k_hydro32t<false, kForcePhi>,
@@ -105,7 +119,7 @@ static cudaError_t hydro32t_prepare() {
                        (const void *)k_hydro32p<true, kForceArrays>, (const void *)k_hydro32p<false, kForceArrays>,
                        (const void *)k_hydro32p<true, kForceNone>, (const void *)k_hydro32p<false, kForceNone>};
   for (const void *f : fns) {
-    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem32t);
+    cudaError_t e = smem_attrs(f, kSmem32t);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -115,7 +129,10 @@ static cudaError_t hydro32t_prepare() {
 // Nu is a multiple of 1024, and the four factored passes fused into one kernel at Nu = 1024
 static bool u_factored(int Nu) { return Nu % 1024 == 0; }
 static bool u_fused(int Nu) { return Nu == 1024; }
+// the forward phi transform as a fused two-stage kernel (phifwd.cuh) when both are 1024
+static bool phi_fused(int Nu, int Nphi) { return Nu == 1024 && Nphi == 1024; }
 
+// K-major BF16 matrix [rows][cols] -> tiles of box_rows x 64 with 128-byte swizzle.
 static bool make_map(CUtensorMap *m, const void *base, uint64_t rows, uint64_t cols, uint32_t box_rows) {
   auto fn = encode_fn();
   if (!fn) return false;
@@ -228,6 +245,31 @@ __global__ void k_tab_kw2(float *KW2, const double2 *khat, int nm, int A, int Np
     const int row = (int)(q / (2 * A)), col = (int)(q % (2 * A));
     const int m = row >> 6, p2 = row & 63, p1 = col >> 1;
     KW2[q] = (m <= Nphi / 2) ? (float)(khat[(size_t)m * M + p2 + 64 * p1].x / M) : 0.f;
+  }
+}
+
+// twiddles of k_phifwd: W_N^{m2 j1} = e^{-2 pi i m2 j1 / N}, [32][32]
+__global__ void k_tab_twphi(float2 *tw, int N) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 32 * 32; q += gridDim.x * blockDim.x) {
+    const int m2 = q / 32, j1 = q % 32;
+    double sn, cs;
+    sincospi(2.0 * (double)(m2 * j1) / N, &sn, &cs);
+    tw[q] = make_float2((float)cs, (float)-sn);
+  }
+}
+
+// stage-A operand of k_phifwd: C[(m2, ro)][j2] = cos / -sin (2 pi m2 j2 / 32), 128 x 64 with
+// rows 64.. and columns 32.. zero
+__global__ void k_tab_phiA(SplitBuf C) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 128 * 64; q += gridDim.x * blockDim.x) {
+    const int r = q / 64, k = q % 64;
+    double v = 0.0;
+    if (r < 64 && k < 32) {
+      double sn, cs;
+      sincospi(2.0 * (double)(((r >> 1) * k) % 32) / 32.0, &sn, &cs);
+      v = (r & 1) ? -sn : cs;
+    }
+    put_split(C, q, v);
   }
 }
 
@@ -476,12 +518,11 @@ static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUte
 template <int MODE, bool A_MN, bool B_MN>
 static cudaError_t prepare_gemm() {
   cudaError_t e;
-  e = cudaFuncSetAttribute(tc::k_gemm_split<MODE, A_MN, B_MN, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::smem_bytes(1));
+  e = smem_attrs((const void *)tc::k_gemm_split<MODE, A_MN, B_MN, 1>, tc::smem_bytes(1));
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(tc::k_gemm_split<MODE, A_MN, B_MN, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::smem_bytes(2));
+  e = smem_attrs((const void *)tc::k_gemm_split<MODE, A_MN, B_MN, 2>, tc::smem_bytes(2));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(tc::k_gemm_split<MODE, A_MN, B_MN, tc::STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)tc::smem_bytes(tc::STAGES));
+  return smem_attrs((const void *)tc::k_gemm_split<MODE, A_MN, B_MN, tc::STAGES>, tc::smem_bytes(tc::STAGES));
 }
 
 int dg_handle::mixed_init() {
@@ -561,7 +602,21 @@ int dg_handle::mixed_init() {
       k_tab_tw<<<64, 256, 0, st>>>(X.twp, A, tc::kUcTwLd);
       k_tab_khm<<<grid_for((size_t)nm * 64 * A), 256, 0, st>>>(X.khm, Khat, nm, 64 * A, Nphi);
       XK(cudaGetLastError());
-      XK(cudaFuncSetAttribute(tc::k_uconv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kUcSmem));
+      XK(smem_attrs((const void *)tc::k_uconv, tc::kUcSmem));
+    }
+    X.fused_phi = X.fused_u && phi_fused(Nu, Nphi);
+    if (X.fused_phi) {
+      XK(alloc_split(X.PA, (size_t)128 * 64));
+      XK(alloc_split(X.PB, (size_t)64 * 64));
+      XK(dalloc(&X.twphi, (size_t)32 * 32));
+      k_tab_phiA<<<32, 256, 0, st>>>(X.PA);
+      k_tab_cblock<<<32, 256, 0, st>>>(X.PB, 32, 32, 32, -1);  // W_32^{m1 j1}
+      k_tab_twphi<<<8, 128, 0, st>>>(X.twphi, Nphi);            // W_Nphi^{m2 j1}
+      XK(cudaGetLastError());
+      bool okp = make_map(&X.mPA[0], X.PA.hi, 128, 64, tc::BM) && make_map(&X.mPA[1], X.PA.lo, 128, 64, tc::BM) &&
+                 make_map(&X.mPB[0], X.PB.hi, 64, 64, tc::BN) && make_map(&X.mPB[1], X.PB.lo, 64, 64, tc::BN);
+      if (!okp) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed (fused phi transform)");
+      XK(smem_attrs((const void *)tc::k_phifwd, tc::kPfSmem));
     }
     bool okf = make_map(&X.mXin[0], X.Xin.hi, 64, (uint64_t)nm * A, 64) && make_map(&X.mXin[1], X.Xin.lo, 64, (uint64_t)nm * A, 64) &&
                make_map(&X.mTb[0], X.Tb.hi, 2 * A, (uint64_t)nm * 64, 64) && make_map(&X.mTb[1], X.Tb.lo, 2 * A, (uint64_t)nm * 64, 64) &&
@@ -615,9 +670,9 @@ void dg_handle::mixed_release() {
     if (X.w[b]) cudaFree(X.w[b]);
   }
   SplitBuf *bufs[] = {&X.Sx, &X.X1, &X.Wt, &X.Z, &X.Fphi, &X.Cu, &X.CuT, &X.Gphi,
-                      &X.Xin, &X.Tb, &X.Yk, &X.Ub, &X.RB, &X.RA, &X.RGA, &X.RGB};
+                      &X.Xin, &X.Tb, &X.Yk, &X.Ub, &X.RB, &X.RA, &X.RGA, &X.RGB, &X.PA, &X.PB};
   for (SplitBuf *b : bufs) free_split(*b);
-  void *ptrs[] = {X.KW, X.dPhi, X.phiscale, X.rowbuf, X.rowbufd, X.KW2, X.tw, X.khm, X.twp};
+  void *ptrs[] = {X.KW, X.dPhi, X.phiscale, X.rowbuf, X.rowbufd, X.KW2, X.tw, X.khm, X.twp, X.twphi};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   delete mx;
@@ -984,7 +1039,14 @@ int dg_handle::mixed_gravity() {
     // G1: phi DFT, stored as the F1 operand Xin[(i2, ri)][(m, i1)]
     a.out_hi = X.Xin.hi; a.out_lo = X.Xin.lo;
     XK(prof_begin(DG_PROF_GRAV_PHI_FWD));
-    XK(gemm<tc::kEpiPhiToXin>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st, X.ns[0]));
+    if (X.fused_phi) {
+      // real 32-point stage, twiddle, complex 32-point stage: 4 rows per CTA
+      tc::PhiFwdArgs f{X.Sx.hi, X.Sx.lo, X.twphi, X.Xin.hi, X.Xin.lo, nm * A, Nphi, &ctl->status};
+      XK(launch_pdl(tc::k_phifwd, dim3(Nu / tc::kPfRows), dim3(tc::kPfThreads), tc::kPfSmem, st, X.mPA[0], X.mPA[1],
+                    X.mPB[0], X.mPB[1], f));
+    } else {
+      XK(gemm<tc::kEpiPhiToXin>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st, X.ns[0]));
+    }
     XK(prof_end(DG_PROF_GRAV_PHI_FWD));
     XK(prof_begin(DG_PROF_GRAV_U));
     if (X.fused_u) {

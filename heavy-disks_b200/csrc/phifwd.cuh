@@ -1,0 +1,202 @@
+// Fused forward phi transform of the split-BF16 gravity, Nphi = 1024 (= 32 x 32), written
+// straight into the operand layout of the fused radial convolution (uconv.cuh).
+//
+// For every radial row i the phi spectrum of the real source x[j] = R^{3/2} sigma is
+//   X[m] = sum_j x[j] W^{jm},  W = e^{-2 pi i / 1024},  m = 0 .. 512
+// (kalnajs.hpp:48-63, the r2c over phi).  With j = j1 + 32 j2 and m = m2 + 32 m1:
+//   SA  Y[j1][m2] = sum_{j2} W_32^{j2 m2} x[j1 + 32 j2]          (real input, 32 points)
+//   SB  X[m2 + 32 m1] = sum_{j1} W_32^{j1 m1} (W^{j1 m2} Y[j1][m2])   (complex, 32 points)
+// Both stages are tcgen05 split-BF16 products (A_hi B_hi + A_hi B_lo + A_lo B_hi, FP32 in
+// TMEM).  One CTA takes 4 rows:
+//   SA: D[(m2, ro)][(i, j1)] = C[(m2, ro)][j2] . x[(i, j1)][j2], M = 128 (64 used), N = 128,
+//       K = 32; every thread copies 16-byte runs of x (8 consecutive j1 of one row and one
+//       j2) into the swizzled MN-major layout: per row pair, 32 K rows (j2) of 64 contiguous
+//       (i, j1) entries;
+//   EA: twiddle W^{j1 m2} (the re / im lanes of a pair trade halves by shuffle) and write
+//       T[(m2, i)][(j1, ri)] K-major into swizzled shared memory;
+//   SB: D[(m2, i)][(m1, ro)] = T . B[(m1, ro)][(j1, ri)], M = 128, N = 64, K = 64;
+//   EB: X[m][i] for m <= 512 -> Xin[(i2, ri)][(m, i1)] (i = i1 + 32 i2), BF16 hi / lo.
+// 256 CTAs at Nu = 1024, 8 warps, 64 KB of shared memory, 128 TMEM columns.
+#pragma once
+
+#include "uconv.cuh"
+
+namespace dg {
+namespace tc {
+
+constexpr int kPfRows = 4;        // radial rows per CTA
+constexpr int kPfThreads = 256;
+constexpr uint32_t kPfC = 0;      // stage-A operand C, 128 rows x 64 K (j2 < 32 used)  hi|lo 32 KB
+constexpr uint32_t kPfX = 32768;  // x slice, MN-major: 2 chunks of 32 K rows x 128 B     hi|lo 16 KB
+constexpr uint32_t kPfB = 49152;  // stage-B operand, 64 rows (m1, ro) x 64 K (j1, ri)     hi|lo 16 KB
+constexpr uint32_t kPfT = 0;      // T, 128 rows (m2, i) x 64 K (j1, ri), over C (dead after SA)
+constexpr size_t kPfSmem = 65536 + 1024;
+constexpr uint32_t kPfTmemCols = 128;
+
+struct PhiFwdArgs {
+  const __nv_bfloat16 *sx_hi, *sx_lo;  // R^{3/2} sigma, [Nu][Nphi]
+  const float2 *twiddle;  // W^{m2 j1}, [32][32]
+  __nv_bfloat16 *xin_hi, *xin_lo;  // Xin[(i2, ri)][(m, i1)], row length ld
+  int ld;                 // nmodes * 32
+  int Nphi;
+  int *status;
+};
+
+__global__ void __launch_bounds__(kPfThreads, 2)
+    k_phifwd(const __grid_constant__ CUtensorMap tCh, const __grid_constant__ CUtensorMap tCl,
+             const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl, PhiFwdArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t *sm = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ __align__(8) uint64_t bar_in, bar_mma;
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = warp & 3, hw = warp >> 2;
+  const int i0 = blockIdx.x * kPfRows;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar_in, 1);
+    mbar_init(&bar_mma, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tmem_alloc(&tmem_slot, kPfTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16);
+  bool in_seen = false;
+
+  // EA's rows (m2, ro) and their 16 twiddles W^{j1 m2}, j1 in [16 ro, 16 ro + 16), loaded now
+  const bool ea = q < 2;  // TMEM lanes 0..63 hold the 64 rows of stage A
+  const int ra = q * 32 + lane, m2a = ra >> 1, roa = ra & 1;
+  float2 tw[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) tw[k] = ea ? __ldg(a.twiddle + m2a * 32 + 16 * roa + k) : make_float2(0.f, 0.f);
+
+  if (threadIdx.x == 0) {  // constant operands: they do not depend on the previous kernel
+    mbar_arrive_expect_tx(&bar_in, 49152);
+    tma_load_2d(sm + kPfC, &tCh, &bar_in, 0, 0);
+    tma_load_2d(sm + kPfC + 16384, &tCl, &bar_in, 0, 0);
+    tma_load_2d(sm + kPfB, &tBh, &bar_in, 0, 0);
+    tma_load_2d(sm + kPfB + 8192, &tBl, &bar_in, 0, 0);
+  }
+  pdl_wait();  // the source comes from the previous kernel (and Xin's last reader is done)
+  pdl_trigger();
+  // x slice: chunk t of a plane = row pair ip, K row j2, 16-byte chunk c of the 128-byte row,
+  // holding x[i0 + 2 ip + c / 4][32 j2 + 8 (c % 4) .. + 7]
+  {
+    uint4 xv[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int t = threadIdx.x + kPfThreads * (r & 1), ip = t >> 8, j2 = (t >> 3) & 31, c = t & 7;
+      const size_t g = (size_t)(i0 + 2 * ip + (c >> 2)) * a.Nphi + 32 * j2 + 8 * (c & 3);
+      xv[r] = *reinterpret_cast<const uint4 *>((r < 2 ? a.sx_hi : a.sx_lo) + g);
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int t = threadIdx.x + kPfThreads * (r & 1), ip = t >> 8, j2 = (t >> 3) & 31, c = t & 7;
+      *reinterpret_cast<uint4 *>(sm + kPfX + (r < 2 ? 0 : 8192) + ip * 4096 + sw128(j2, c)) = xv[r];
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    in_seen = mbar_wait(&bar_in, 0, a.status);
+    if (in_seen) {
+      tc_fence_after();
+      // ---- SA: D[(m2, ro)][(i, j1)], TMEM columns 0..127 ----
+      const uint32_t id = idesc_bf16(128, 128, false, true);
+      const uint64_t ah = sdesc_sw128(sm + kPfC), al = sdesc_sw128(sm + kPfC + 16384);
+      const uint64_t bh = sdesc_mn_sw128(sm + kPfX, 4096), bl = sdesc_mn_sw128(sm + kPfX + 8192, 4096);
+#pragma unroll
+      for (int kk = 0; kk < 2; ++kk) mma3(tmem, ah + 2 * kk, al + 2 * kk, bh + 128 * kk, bl + 128 * kk, id, kk == 0);
+      mma_commit(&bar_mma);
+    } else {
+      abort_flag = 1;
+    }
+  }
+  __syncwarp();
+  bool ok = mbar_wait(&bar_mma, 0, a.status);
+  tc_fence_after();
+
+  // ---- EA: twiddle; T[(m2, i)][(j1, ri)] (row 4 m2 + i, K-major, swizzled) ----
+  if (__all_sync(0xffffffffu, ok && !abort_flag)) {  // warp-uniform: tcgen05.ld is .sync.aligned
+    if (ea) {
+#pragma unroll 1
+      for (int ii = 0; ii < 2; ++ii) {
+        const int il = 2 * hw + ii;
+        uint32_t v[32];
+        tmem_ld32(tl + (uint32_t)(il * 32), v);  // columns (il, j1), j1 = 0..31
+        const int R = 4 * m2a + il;
+        uint32_t ph[16], pl[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          // the re lane (ro = 0) takes j1 = k, the im lane j1 = 16 + k
+          const float lo_half = __uint_as_float(v[k]), hi_half = __uint_as_float(v[16 + k]);
+          const float recv = __shfl_xor_sync(0xffffffffu, roa ? lo_half : hi_half, 1);
+          const float re = roa ? recv : lo_half, im = roa ? hi_half : recv;
+          const float tr = re * tw[k].x - im * tw[k].y, ti = re * tw[k].y + im * tw[k].x;
+          split_pair(tr, ti, ph[k], pl[k]);
+        }
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {  // K chunk 4 ro + g holds j1 = 16 ro + 4 g .. + 3
+          const uint32_t off = sw128(R, 4 * roa + g);
+          *reinterpret_cast<uint4 *>(sm + kPfT + off) = make_uint4(ph[4 * g], ph[4 * g + 1], ph[4 * g + 2], ph[4 * g + 3]);
+          *reinterpret_cast<uint4 *>(sm + kPfT + 16384 + off) =
+              make_uint4(pl[4 * g], pl[4 * g + 1], pl[4 * g + 2], pl[4 * g + 3]);
+        }
+      }
+    }
+  } else {
+    abort_flag = 1;
+  }
+  uc_stage_sync();
+
+  // ---- SB: D[(m2, i)][(m1, ro)], TMEM columns 0..63 ----
+  if (threadIdx.x == 0 && !abort_flag) {
+    const uint32_t id = idesc_bf16(128, 64);
+    const uint64_t ah = sdesc_sw128(sm + kPfT), al = sdesc_sw128(sm + kPfT + 16384);
+    const uint64_t bh = sdesc_sw128(sm + kPfB), bl = sdesc_sw128(sm + kPfB + 8192);
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) mma3(tmem, ah + 2 * kk, al + 2 * kk, bh + 2 * kk, bl + 2 * kk, id, kk == 0);
+    mma_commit(&bar_mma);
+  }
+  __syncwarp();
+  ok = !abort_flag && mbar_wait(&bar_mma, 1, a.status);
+  tc_fence_after();
+
+  // ---- EB: X[m2 + 32 m1][i] -> Xin[(i2, ri)][(m, i1)] for m <= Nphi / 2 ----
+  if (__all_sync(0xffffffffu, ok && !abort_flag)) {
+    uint32_t v[32];
+    tmem_ld32(tl + (uint32_t)(32 * hw), v);  // columns (m1, ro), m1 = 16 hw .. 16 hw + 15
+    const int rb = q * 32 + lane, m2 = rb >> 2, il = rb & 3;
+    const int i = i0 + il, i1 = i & 31, i2 = i >> 5;
+    const int half = a.Nphi / 2;
+    const size_t rre = (size_t)(2 * i2) * a.ld, rim = rre + a.ld;
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const int m = m2 + 32 * (16 * hw + t);
+      if (m <= half) {
+        const size_t col = (size_t)m * 32 + i1;
+        __nv_bfloat16 h, l;
+        split_bf16(__uint_as_float(v[2 * t]), h, l);
+        a.xin_hi[rre + col] = h;
+        a.xin_lo[rre + col] = l;
+        if (m != 0 && m != half) {  // self-conjugate modes have no imaginary part
+          split_bf16(__uint_as_float(v[2 * t + 1]), h, l);
+          a.xin_hi[rim + col] = h;
+          a.xin_lo[rim + col] = l;
+        }
+      }
+    }
+  }
+  if (threadIdx.x == 0 && !in_seen) mbar_wait(&bar_in, 0, a.status);  // copies in flight land first
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kPfTmemCols);
+}
+
+}  // namespace tc
+}  // namespace dg
