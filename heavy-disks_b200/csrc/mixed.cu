@@ -258,13 +258,13 @@ __global__ void k_tab_twphi(float2 *tw, int N) {
   }
 }
 
-// stage-A operand of k_phifwd: C[(m2, ro)][j2] = cos / -sin (2 pi m2 j2 / 32), 128 x 64 with
-// rows 64.. and columns 32.. zero
+// stage-A operand of k_phifwd: C[(m2, ro)][j2] = cos / -sin (2 pi m2 j2 / 32), 64 x 64 with
+// columns 32.. zero
 __global__ void k_tab_phiA(SplitBuf C) {
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 128 * 64; q += gridDim.x * blockDim.x) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 64 * 64; q += gridDim.x * blockDim.x) {
     const int r = q / 64, k = q % 64;
     double v = 0.0;
-    if (r < 64 && k < 32) {
+    if (k < 32) {
       double sn, cs;
       sincospi(2.0 * (double)(((r >> 1) * k) % 32) / 32.0, &sn, &cs);
       v = (r & 1) ? -sn : cs;
@@ -606,14 +606,14 @@ int dg_handle::mixed_init() {
     }
     X.fused_phi = X.fused_u && phi_fused(Nu, Nphi);
     if (X.fused_phi) {
-      XK(alloc_split(X.PA, (size_t)128 * 64));
+      XK(alloc_split(X.PA, (size_t)64 * 64));
       XK(alloc_split(X.PB, (size_t)64 * 64));
       XK(dalloc(&X.twphi, (size_t)32 * 32));
       k_tab_phiA<<<32, 256, 0, st>>>(X.PA);
       k_tab_cblock<<<32, 256, 0, st>>>(X.PB, 32, 32, 32, -1);  // W_32^{m1 j1}
       k_tab_twphi<<<8, 128, 0, st>>>(X.twphi, Nphi);            // W_Nphi^{m2 j1}
       XK(cudaGetLastError());
-      bool okp = make_map(&X.mPA[0], X.PA.hi, 128, 64, tc::BM) && make_map(&X.mPA[1], X.PA.lo, 128, 64, tc::BM) &&
+      bool okp = make_map(&X.mPA[0], X.PA.hi, 64, 64, tc::BN) && make_map(&X.mPA[1], X.PA.lo, 64, 64, tc::BN) &&
                  make_map(&X.mPB[0], X.PB.hi, 64, 64, tc::BN) && make_map(&X.mPB[1], X.PB.lo, 64, 64, tc::BN);
       if (!okp) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed (fused phi transform)");
       XK(smem_attrs((const void *)tc::k_phifwd, tc::kPfSmem));

@@ -8,15 +8,16 @@
 //   SB  X[m2 + 32 m1] = sum_{j1} W_32^{j1 m1} (W^{j1 m2} Y[j1][m2])   (complex, 32 points)
 // Both stages are tcgen05 split-BF16 products (A_hi B_hi + A_hi B_lo + A_lo B_hi, FP32 in
 // TMEM).  One CTA takes 4 rows:
-//   SA: D[(m2, ro)][(i, j1)] = C[(m2, ro)][j2] . x[(i, j1)][j2], M = 128 (64 used), N = 128,
-//       K = 32; every thread copies 16-byte runs of x (8 consecutive j1 of one row and one
-//       j2) into the swizzled MN-major layout: per row pair, 32 K rows (j2) of 64 contiguous
-//       (i, j1) entries;
-//   EA: twiddle W^{j1 m2} (the re / im lanes of a pair trade halves by shuffle) and write
-//       T[(m2, i)][(j1, ri)] K-major into swizzled shared memory;
+//   SA: D[(i, j1)][(m2, ro)] = x[(i, j1)][j2] . C[(m2, ro)][j2], M = 128, N = 64, K = 32;
+//       every thread copies 16-byte runs of x (8 consecutive j1 of one row and one j2) into
+//       the swizzled MN-major layout: per row pair, 32 K rows (j2) of 64 contiguous (i, j1)
+//       entries;
+//   EA: each TMEM lane (i, j1) holds its complex Y[m2] in column pairs: twiddle W^{j1 m2}
+//       and write T[(m2, i)][(j1, ri)] K-major into swizzled shared memory (a warp, one i,
+//       fills 128 contiguous bytes of a row);
 //   SB: D[(m2, i)][(m1, ro)] = T . B[(m1, ro)][(j1, ri)], M = 128, N = 64, K = 64;
 //   EB: X[m][i] for m <= 512 -> Xin[(i2, ri)][(m, i1)] (i = i1 + 32 i2), BF16 hi / lo.
-// 256 CTAs at Nu = 1024, 8 warps, 64 KB of shared memory, 128 TMEM columns.
+// 256 CTAs at Nu = 1024, 8 warps, 48 KB of shared memory, 128 TMEM columns.
 #pragma once
 
 #include "uconv.cuh"
@@ -26,11 +27,11 @@ namespace tc {
 
 constexpr int kPfRows = 4;        // radial rows per CTA
 constexpr int kPfThreads = 256;
-constexpr uint32_t kPfC = 0;      // stage-A operand C, 128 rows x 64 K (j2 < 32 used)  hi|lo 32 KB
-constexpr uint32_t kPfX = 32768;  // x slice, MN-major: 2 chunks of 32 K rows x 128 B     hi|lo 16 KB
-constexpr uint32_t kPfB = 49152;  // stage-B operand, 64 rows (m1, ro) x 64 K (j1, ri)     hi|lo 16 KB
-constexpr uint32_t kPfT = 0;      // T, 128 rows (m2, i) x 64 K (j1, ri), over C (dead after SA)
-constexpr size_t kPfSmem = 65536 + 1024;
+constexpr uint32_t kPfC = 0;      // stage-A operand C, 64 rows (m2, ro) x 64 K (j2 < 32 used) hi|lo 16 KB
+constexpr uint32_t kPfX = 16384;  // x slice, MN-major: 2 chunks of 32 K rows x 128 B          hi|lo 16 KB
+constexpr uint32_t kPfB = 32768;  // stage-B operand, 64 rows (m1, ro) x 64 K (j1, ri)          hi|lo 16 KB
+constexpr uint32_t kPfT = 0;      // T, 128 rows (m2, i) x 64 K (j1, ri), over C and x (dead after SA) hi|lo 32 KB
+constexpr size_t kPfSmem = 49152 + 1024;
 constexpr uint32_t kPfTmemCols = 128;
 
 struct PhiFwdArgs {
@@ -68,17 +69,16 @@ __global__ void __launch_bounds__(kPfThreads, 2)
   const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16);
   bool in_seen = false;
 
-  // EA's rows (m2, ro) and their 16 twiddles W^{j1 m2}, j1 in [16 ro, 16 ro + 16), loaded now
-  const bool ea = q < 2;  // TMEM lanes 0..63 hold the 64 rows of stage A
-  const int ra = q * 32 + lane, m2a = ra >> 1, roa = ra & 1;
+  // EA: TMEM lane (i = q, j1 = lane), columns m2 in [16 hw, 16 hw + 16); their twiddles
+  // W^{j1 m2} are loaded now
   float2 tw[16];
 #pragma unroll
-  for (int k = 0; k < 16; ++k) tw[k] = ea ? __ldg(a.twiddle + m2a * 32 + 16 * roa + k) : make_float2(0.f, 0.f);
+  for (int k = 0; k < 16; ++k) tw[k] = __ldg(a.twiddle + (16 * hw + k) * 32 + lane);
 
   if (threadIdx.x == 0) {  // constant operands: they do not depend on the previous kernel
-    mbar_arrive_expect_tx(&bar_in, 49152);
+    mbar_arrive_expect_tx(&bar_in, 32768);
     tma_load_2d(sm + kPfC, &tCh, &bar_in, 0, 0);
-    tma_load_2d(sm + kPfC + 16384, &tCl, &bar_in, 0, 0);
+    tma_load_2d(sm + kPfC + 8192, &tCl, &bar_in, 0, 0);
     tma_load_2d(sm + kPfB, &tBh, &bar_in, 0, 0);
     tma_load_2d(sm + kPfB + 8192, &tBl, &bar_in, 0, 0);
   }
@@ -106,12 +106,12 @@ __global__ void __launch_bounds__(kPfThreads, 2)
     in_seen = mbar_wait(&bar_in, 0, a.status);
     if (in_seen) {
       tc_fence_after();
-      // ---- SA: D[(m2, ro)][(i, j1)], TMEM columns 0..127 ----
-      const uint32_t id = idesc_bf16(128, 128, false, true);
-      const uint64_t ah = sdesc_sw128(sm + kPfC), al = sdesc_sw128(sm + kPfC + 16384);
-      const uint64_t bh = sdesc_mn_sw128(sm + kPfX, 4096), bl = sdesc_mn_sw128(sm + kPfX + 8192, 4096);
+      // ---- SA: D[(i, j1)][(m2, ro)], TMEM columns 0..63 ----
+      const uint32_t id = idesc_bf16(128, 64, true, false);
+      const uint64_t ah = sdesc_mn_sw128(sm + kPfX, 4096), al = sdesc_mn_sw128(sm + kPfX + 8192, 4096);
+      const uint64_t bh = sdesc_sw128(sm + kPfC), bl = sdesc_sw128(sm + kPfC + 8192);
 #pragma unroll
-      for (int kk = 0; kk < 2; ++kk) mma3(tmem, ah + 2 * kk, al + 2 * kk, bh + 128 * kk, bl + 128 * kk, id, kk == 0);
+      for (int kk = 0; kk < 2; ++kk) mma3(tmem, ah + 128 * kk, al + 128 * kk, bh + 2 * kk, bl + 2 * kk, id, kk == 0);
       mma_commit(&bar_mma);
     } else {
       abort_flag = 1;
@@ -123,44 +123,31 @@ __global__ void __launch_bounds__(kPfThreads, 2)
 
   // ---- EA: twiddle; T[(m2, i)][(j1, ri)] (row 4 m2 + i, K-major, swizzled) ----
   if (__all_sync(0xffffffffu, ok && !abort_flag)) {  // warp-uniform: tcgen05.ld is .sync.aligned
-    if (ea) {
-#pragma unroll 1
-      for (int ii = 0; ii < 2; ++ii) {
-        const int il = 2 * hw + ii;
-        uint32_t v[32];
-        tmem_ld32(tl + (uint32_t)(il * 32), v);  // columns (il, j1), j1 = 0..31
-        const int R = 4 * m2a + il;
-        uint32_t ph[16], pl[16];
+    uint32_t v[32];
+    tmem_ld32(tl + (uint32_t)(32 * hw), v);  // columns (m2, ro), m2 = 16 hw .. 16 hw + 15
+    const int il = q, j1 = lane;
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          // the re lane (ro = 0) takes j1 = k, the im lane j1 = 16 + k
-          const float lo_half = __uint_as_float(v[k]), hi_half = __uint_as_float(v[16 + k]);
-          const float recv = __shfl_xor_sync(0xffffffffu, roa ? lo_half : hi_half, 1);
-          const float re = roa ? recv : lo_half, im = roa ? hi_half : recv;
-          const float tr = re * tw[k].x - im * tw[k].y, ti = re * tw[k].y + im * tw[k].x;
-          split_pair(tr, ti, ph[k], pl[k]);
-        }
-#pragma unroll
-        for (int g = 0; g < 4; ++g) {  // K chunk 4 ro + g holds j1 = 16 ro + 4 g .. + 3
-          const uint32_t off = sw128(R, 4 * roa + g);
-          *reinterpret_cast<uint4 *>(sm + kPfT + off) = make_uint4(ph[4 * g], ph[4 * g + 1], ph[4 * g + 2], ph[4 * g + 3]);
-          *reinterpret_cast<uint4 *>(sm + kPfT + 16384 + off) =
-              make_uint4(pl[4 * g], pl[4 * g + 1], pl[4 * g + 2], pl[4 * g + 3]);
-        }
-      }
+    for (int t = 0; t < 16; ++t) {
+      const float re = __uint_as_float(v[2 * t]), im = __uint_as_float(v[2 * t + 1]);
+      const float tr = re * tw[t].x - im * tw[t].y, ti = re * tw[t].y + im * tw[t].x;
+      uint32_t hi, lo;
+      split_pair(tr, ti, hi, lo);
+      const uint32_t off = sw128(4 * (16 * hw + t) + il, j1 >> 2) + (uint32_t)(j1 & 3) * 4;
+      *reinterpret_cast<uint32_t *>(sm + kPfT + off) = hi;
+      *reinterpret_cast<uint32_t *>(sm + kPfT + 16384 + off) = lo;
     }
   } else {
     abort_flag = 1;
   }
   uc_stage_sync();
 
-  // ---- SB: D[(m2, i)][(m1, ro)], TMEM columns 0..63 ----
+  // ---- SB: D[(m2, i)][(m1, ro)], TMEM columns 64..127 ----
   if (threadIdx.x == 0 && !abort_flag) {
     const uint32_t id = idesc_bf16(128, 64);
     const uint64_t ah = sdesc_sw128(sm + kPfT), al = sdesc_sw128(sm + kPfT + 16384);
     const uint64_t bh = sdesc_sw128(sm + kPfB), bl = sdesc_sw128(sm + kPfB + 8192);
 #pragma unroll
-    for (int kk = 0; kk < 4; ++kk) mma3(tmem, ah + 2 * kk, al + 2 * kk, bh + 2 * kk, bl + 2 * kk, id, kk == 0);
+    for (int kk = 0; kk < 4; ++kk) mma3(tmem + 64, ah + 2 * kk, al + 2 * kk, bh + 2 * kk, bl + 2 * kk, id, kk == 0);
     mma_commit(&bar_mma);
   }
   __syncwarp();
@@ -170,7 +157,7 @@ __global__ void __launch_bounds__(kPfThreads, 2)
   // ---- EB: X[m2 + 32 m1][i] -> Xin[(i2, ri)][(m, i1)] for m <= Nphi / 2 ----
   if (__all_sync(0xffffffffu, ok && !abort_flag)) {
     uint32_t v[32];
-    tmem_ld32(tl + (uint32_t)(32 * hw), v);  // columns (m1, ro), m1 = 16 hw .. 16 hw + 15
+    tmem_ld32(tl + (uint32_t)(64 + 32 * hw), v);  // columns (m1, ro), m1 = 16 hw .. 16 hw + 15
     const int rb = q * 32 + lane, m2 = rb >> 2, il = rb & 3;
     const int i = i0 + il, i1 = i & 31, i2 = i >> 5;
     const int half = a.Nphi / 2;
