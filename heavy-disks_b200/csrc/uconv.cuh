@@ -149,15 +149,17 @@ __global__ void __launch_bounds__(kUcThreads, 1)
     tma_load_2d(sm + kUcX + 8192, &tXh, &bar_in0, x0 + 64, 0);
     tma_load_2d(sm + kUcX + 16384, &tXl, &bar_in0, x0, 0);
     tma_load_2d(sm + kUcX + 24576, &tXl, &bar_in0, x0 + 64, 0);
-    // ---- S1: D1[(p2, ro)][(m, i1)] at TMEM columns 0..127 ----
+    // ---- S1: D1[(m, i1)][(p2, ro)] at TMEM columns 0..127 (the input slice is the A
+    // operand, MN-major, so every TMEM lane is one (mode, i1) and its (re, im) pairs sit
+    // in adjacent columns) ----
     in0_seen = mbar_wait(&bar_in0, 0, a.status);
     if (in0_seen) {
       tc_fence_after();
-      const uint32_t id = idesc_bf16(128, 128, false, true);
-      const uint64_t ah = sdesc_sw128(sm + kUcRB), al = sdesc_sw128(sm + kUcRB + 16384);
-      const uint64_t bh = sdesc_mn_sw128(sm + kUcX, 8192), bl = sdesc_mn_sw128(sm + kUcX + 16384, 8192);
+      const uint32_t id = idesc_bf16(128, 128, true, false);
+      const uint64_t ah = sdesc_mn_sw128(sm + kUcX, 8192), al = sdesc_mn_sw128(sm + kUcX + 16384, 8192);
+      const uint64_t bh = sdesc_sw128(sm + kUcRB), bl = sdesc_sw128(sm + kUcRB + 16384);
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk) mma3(tmem, ah + 2 * kk, al + 2 * kk, bh + 128 * kk, bl + 128 * kk, id, kk == 0);
+      for (int kk = 0; kk < 4; ++kk) mma3(tmem, ah + 128 * kk, al + 128 * kk, bh + 2 * kk, bl + 2 * kk, id, kk == 0);
       mma_commit(&bar_mma);
     } else {
       abort_flag = 1;
@@ -172,27 +174,22 @@ __global__ void __launch_bounds__(kUcThreads, 1)
   // ---- E1: twiddle W_M^{i1 p2}; T[(m, p2)][(i1, ri)] ----
   ok = ok && !abort_flag && mbar_wait(&bar_in0, 0, a.status);  // the twiddles in shared memory, for every thread
   if (__all_sync(0xffffffffu, ok && !abort_flag)) {  // warp-uniform: tcgen05.ld is .sync.aligned
-    const int r1 = q * 32 + lane, p21 = r1 >> 1, ro = r1 & 1;
-    float2 w[16];
-#pragma unroll
-    for (int j = 0; j < 16; ++j) w[j] = tws[p21 * kUcTwLd + 2 * j + ro];  // i1 = 2 j + ro
+    // lane (m = q, i1 = lane); columns (p2, ro) for p2 in [32 hw, 32 hw + 32)
+    const int i1 = lane;
 #pragma unroll 1
-    for (int mj = 0; mj < 2; ++mj) {
-      const int mlj = 2 * hw + mj;
+    for (int c = 0; c < 2; ++c) {
       uint32_t v[32];
-      tmem_ld32(tl + (uint32_t)(mlj * 32), v);
-      const int R = mlj * 64 + p21;
+      tmem_ld32(tl + (uint32_t)(64 * hw + 32 * c), v);
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        // lanes (p2, re) and (p2, im) trade halves: the re lane takes i1 = 2j, the im lane 2j+1
-        const float x0 = __uint_as_float(v[2 * j]), x1 = __uint_as_float(v[2 * j + 1]);
-        const float recv = __shfl_xor_sync(0xffffffffu, ro ? x0 : x1, 1);
-        const float re = ro ? recv : x0, im = ro ? x1 : recv;
-        const int i1 = 2 * j + ro;
-        const float tr = re * w[j].x - im * w[j].y, ti = re * w[j].y + im * w[j].x;
+      for (int t = 0; t < 16; ++t) {
+        const int p2 = 32 * hw + 16 * c + t;
+        const float re = __uint_as_float(v[2 * t]), im = __uint_as_float(v[2 * t + 1]);
+        const float2 w = tws[p2 * kUcTwLd + i1];
+        const float tr = re * w.x - im * w.y, ti = re * w.y + im * w.x;
         uint32_t hi, lo;
         split_pair(tr, ti, hi, lo);
-        const uint32_t off = sw128(R, i1 >> 2) + (uint32_t)(i1 & 3) * 4;
+        // row (m, p2) of T; the warp's 32 lanes fill its 128 bytes
+        const uint32_t off = sw128(q * 64 + p2, i1 >> 2) + (uint32_t)(i1 & 3) * 4;
         *reinterpret_cast<uint32_t *>(sm + kUcT + off) = hi;
         *reinterpret_cast<uint32_t *>(sm + kUcT + 32768 + off) = lo;
       }
