@@ -428,8 +428,17 @@ def main():
         e["bytes_alg_per_launch" if unit_kind == "B" else "flops_executed_per_launch"] = work
         return e
 
-    hyd_name = "fused hydro sweep (k_hydro32t: 16 x 58 tiles, source + R sweep + phi sweep + CFL)" \
-        if a.precision == "mixed" else "fused hydro sweep (k_hydro64: source + R sweep + phi sweep + CFL)"
+    if a.precision == "mixed":
+        tuned = disk.tuning()
+        form = next((f for f in ("packed", "tile", "warp") if ("hydro " + f) in tuned), "tile")
+        hyd_name = {
+            "packed": "fused hydro sweep (k_hydro32p: 16 x 56 tiles, TMA-staged fields, FP32x2 column pairs, "
+                      "source + R sweep + phi sweep + CFL)",
+            "tile": "fused hydro sweep (k_hydro32t: 16 x 58 tiles, source + R sweep + phi sweep + CFL)",
+            "warp": "fused hydro sweep (k_hydro32w: warp-marching rows, source + R sweep + phi sweep + CFL)",
+        }[form]
+    else:
+        hyd_name = "fused hydro sweep (k_hydro64: source + R sweep + phi sweep + CFL)"
     roof_all = [entry("hydro", hyd_name, "hbm", hyd_bytes, "B")]
     for ph, kern, bound, work, kind in gravity_parts(a.precision, N, N):
         e = entry(ph, kern, bound, work, kind)

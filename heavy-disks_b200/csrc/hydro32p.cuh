@@ -10,9 +10,15 @@
 // neighbours (columns 2l - 2 .. 2l + 2) come from the neighbouring lanes by shuffle.
 // Columns whose results are never used (lanes 0 and 31 in the sweeps) are computed
 // anyway and discarded, so shuffles run with every lane active.
+//
+// Interior column tiles (no periodic wrap inside the tile) with self-gravity or no force
+// stage sigma, u, w and dPhi in shared memory as one TMA box each (64 x 22 floats, rows
+// outside the grid read as zero); the two edge tiles and the caller-forces path use
+// thread loads.
 #pragma once
 
 #include "hydro32t.cuh"
+#include "tc_gemm.cuh"
 
 namespace dg {
 
@@ -23,6 +29,15 @@ constexpr int kItSrcP = (kSrcRows32t + kWarps32p - 1) / kWarps32p;
 constexpr int kItFaceP = (kFaceRows32t + kWarps32p - 1) / kWarps32p;
 constexpr int kItOutP = (kTileI + kWarps32p - 1) / kWarps32p;
 static_assert(kItOutP * kWarps32p == kTileI, "output rows split evenly over the warps");
+// shared-memory plan of this kernel in floats: the five staged fields first (each one TMA
+// box, 16-byte aligned), then the radial fluxes and the row constants.  u1 / w1 (source rows
+// i0-2 ..) overwrite the raw u / w of the same points one row down, in place.
+constexpr int kFieldP = kRows32t * kLd32t;  // 22 x 64
+constexpr int kOffSgP = 0, kOffDpP = kFieldP, kOffPhP = 2 * kFieldP, kOffU0P = 3 * kFieldP, kOffW0P = 4 * kFieldP;
+constexpr int kOffFP = 5 * kFieldP;
+constexpr int kOffRcP = kOffFP + 4 * kFaceArr32t;
+constexpr size_t kSmem32p = (size_t)(kOffRcP + tNConst * kRows32t) * sizeof(float) + 128;  // + alignment slack
+constexpr uint32_t kFieldBytesP = kFieldP * 4;
 
 namespace p2 {
 typedef float2 F2;
@@ -52,15 +67,17 @@ __device__ __forceinline__ void hydro32p_tile(
     const float *__restrict__ sig, const float *__restrict__ uu, const float *__restrict__ ww,
     const float *__restrict__ Phi, const double *__restrict__ gRin, const double *__restrict__ gpin,
     float *__restrict__ so, float *__restrict__ uo, float *__restrict__ wo, const SplitBf16 &Sx, Ctl *ctl,
-    const Rows32 &g, float *sm32t, double *red, double *bsum, double *zsum) {
+    const Rows32 &g, float *sm32t, double *red, double *bsum, double *zsum, const CUtensorMap *tmS,
+    const CUtensorMap *tmU, const CUtensorMap *tmW, const CUtensorMap *tmP, uint64_t *bar_ld) {
   using namespace p2;
-  float *rc = sm32t + kOffRc32t;
+  float *rc = sm32t + kOffRcP;
   // shared arrays as pairs: row r, lane l -> element r * 32 + l
   constexpr int L2 = kLd32t / 2;
-  F2 *SG = reinterpret_cast<F2 *>(sm32t + kOffSg32t), *DP = reinterpret_cast<F2 *>(sm32t + kOffDp32t);
-  F2 *PH = reinterpret_cast<F2 *>(sm32t + kOffPh32t);
-  F2 *U1 = reinterpret_cast<F2 *>(sm32t + kOffU132t), *W1 = reinterpret_cast<F2 *>(sm32t + kOffW132t);
-  F2 *FF = reinterpret_cast<F2 *>(sm32t + kOffF32t), *FR = FF + kFaceArr32t / 2, *GA = FR + kFaceArr32t / 2,
+  F2 *SG = reinterpret_cast<F2 *>(sm32t + kOffSgP), *DP = reinterpret_cast<F2 *>(sm32t + kOffDpP);
+  F2 *PH = reinterpret_cast<F2 *>(sm32t + kOffPhP);
+  F2 *U0 = reinterpret_cast<F2 *>(sm32t + kOffU0P), *W0 = reinterpret_cast<F2 *>(sm32t + kOffW0P);
+  F2 *U1 = U0 + L2, *W1 = W0 + L2;  // source row rs = stored row rs + 1
+  F2 *FF = reinterpret_cast<F2 *>(sm32t + kOffFP), *FR = FF + kFaceArr32t / 2, *GA = FR + kFaceArr32t / 2,
      *GB = GA + kFaceArr32t / 2;
   F2 *U2 = DP, *W2 = PH;            // S4 outputs over the dead source inputs
   F2 *PF = FF, *PR = FR, *PG = GA;  // S5 outputs over the dead radial fluxes
@@ -141,34 +158,52 @@ __device__ __forceinline__ void hydro32p_tile(
     return;
   }
 
-  // ---- S0: every global load first (pairs, 8-byte aligned) ----
-  F2 ur[kItSrcP], wr[kItSrcP], sv[kItLoadP], pv[kItLoadP];
+  // ---- S0: sigma, u, w, dPhi of rows i0-3 .. i0+kTileI+2 into shared memory ----
+  const bool use_tma = FM != kForceArrays && j0 >= 4 && j0 - 4 + kLd32t <= Nphi;  // CTA-uniform
+  if (use_tma) {
+    if (tid == 0) {
+      tc::mbar_arrive_expect_tx(bar_ld, (FM == kForcePhi ? 4u : 3u) * kFieldBytesP);
+      tc::tma_load_2d(sm32t + kOffSgP, tmS, bar_ld, j0 - 4, ib);
+      tc::tma_load_2d(sm32t + kOffU0P, tmU, bar_ld, j0 - 4, ib);
+      tc::tma_load_2d(sm32t + kOffW0P, tmW, bar_ld, j0 - 4, ib);
+      if (FM == kForcePhi) tc::tma_load_2d(sm32t + kOffPhP, tmP, bar_ld, j0 - 4, ib);
+    }
+  } else {
+    F2 sv[kItLoadP], pv[kItLoadP], uv[kItLoadP], wv[kItLoadP];
 #pragma unroll
-  for (int k = 0; k < kItSrcP; ++k) {
-    const int rs = wp + kWarps32p * k, i = ib + 1 + rs;
-    ur[k] = wr[k] = S(0.f);
-    if (rs < kSrcRows32t && row_ok(i)) {
-      const size_t q = (size_t)i * Nphi + jc;
-      ur[k] = *reinterpret_cast<const F2 *>(uu + q);
-      wr[k] = *reinterpret_cast<const F2 *>(ww + q);
+    for (int k = 0; k < kItLoadP; ++k) {
+      const int r = wp + kWarps32p * k, i = ib + r;
+      sv[k] = pv[k] = uv[k] = wv[k] = S(0.f);
+      if (r < kRows32t && row_ok(i)) {
+        const size_t q = (size_t)i * Nphi + jc;
+        sv[k] = *reinterpret_cast<const F2 *>(sig + q);
+        uv[k] = *reinterpret_cast<const F2 *>(uu + q);
+        wv[k] = *reinterpret_cast<const F2 *>(ww + q);
+        if (FM == kForcePhi) pv[k] = *reinterpret_cast<const F2 *>(Phi + q);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kItLoadP; ++k) {
+      const int r = wp + kWarps32p * k;
+      if (r < kRows32t) {
+        SG[r * L2 + lane] = sv[k];
+        U0[r * L2 + lane] = uv[k];
+        W0[r * L2 + lane] = wv[k];
+        PH[r * L2 + lane] = pv[k];
+      }
     }
   }
-#pragma unroll
-  for (int k = 0; k < kItLoadP; ++k) {
-    const int r = wp + kWarps32p * k, i = ib + r;
-    sv[k] = pv[k] = S(0.f);
-    if (r < kRows32t && row_ok(i)) {
-      const size_t q = (size_t)i * Nphi + jc;
-      sv[k] = *reinterpret_cast<const F2 *>(sig + q);
-      if (FM == kForcePhi) pv[k] = *reinterpret_cast<const F2 *>(Phi + q);
-    }
+  __syncthreads();  // row constants (and thread-loaded fields) staged
+  if (use_tma && !tc::mbar_wait(bar_ld, 0, &ctl->status)) {
+    // the copies did not land in time: the step is void (status raised); wait once more
+    // (bounded) so that no copy is in flight when the CTA exits, then go on with the rest
+    if (tid == 0) tc::mbar_wait(bar_ld, 0, &ctl->status);
   }
-  __syncthreads();  // row constants staged
 #pragma unroll
   for (int k = 0; k < kItLoadP; ++k) {
     const int r = wp + kWarps32p * k, i = ib + r;
     if (r < kRows32t) {
-      const F2 s = sv[k];
+      const F2 s = SG[r * L2 + lane];
       F2 d = S(0.f);
       if (row_ok(i)) {
         if (G2) {
@@ -178,9 +213,7 @@ __device__ __forceinline__ void hydro32p_tile(
           d = make_float2(P0 * expm1f(g.gamma * log1pf(s.x * iS0)), P0 * expm1f(g.gamma * log1pf(s.y * iS0)));
         }
       }
-      SG[r * L2 + lane] = s;
       DP[r * L2 + lane] = d;
-      PH[r * L2 + lane] = pv[k];
     }
   }
   __syncthreads();
@@ -223,7 +256,7 @@ __device__ __forceinline__ void hydro32p_tile(
           dgR = make_float2((float)gRin[q], (float)gRin[q + 1]);
           dgp = make_float2((float)gpin[q], (float)gpin[q + 1]);
         }
-        const F2 uc = ur[k], wc = wr[k];
+        const F2 uc = U0[x], wc = W0[x];  // raw u, w of the point (row r of the staged fields)
         const float V = RC(tV0, i);
         const F2 q1 = fdiv(sub(mul(mul(S(RC(tDP0, i)), s_g), S(RC(tInvS0, i))), ddP), s);
         const F2 aR = add(add(add(S(RC(tA0, i)), q1), dgR), mul(mul(add(S(2.f * V), wc), wc), S(iR)));
@@ -449,18 +482,30 @@ __device__ __forceinline__ void hydro32p_tile(
 }
 
 template <bool G2, int FM>
-__global__ void __launch_bounds__(kThreads32t, 3) k_hydro32p(
+__global__ void __launch_bounds__(kThreads32t, 4) k_hydro32p(
+    const __grid_constant__ CUtensorMap tmS, const __grid_constant__ CUtensorMap tmU,
+    const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUtensorMap tmP,
     const float *__restrict__ sig, const float *__restrict__ uu, const float *__restrict__ ww,
     const float *__restrict__ Phi, const double *__restrict__ gRin, const double *__restrict__ gpin,
     float *__restrict__ so, float *__restrict__ uo, float *__restrict__ wo, SplitBf16 Sx, Ctl *ctl, Rows32 g) {
-  extern __shared__ float sm32t[];
+  extern __shared__ __align__(16) uint8_t sm32p_raw[];
+  // TMA destinations: the field offsets are multiples of 128 bytes from a 128-aligned base
+  float *sm32t = reinterpret_cast<float *>(((uintptr_t)sm32p_raw + 127) & ~(uintptr_t)127);
   __shared__ double red[kThreads32t / 32];
   __shared__ double bsum[2 * kMaxModes], zsum[2 * kMaxModes];
+  __shared__ __align__(8) uint64_t bar_ld;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&bar_ld, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // (the first CTA barrier inside the tile function orders the set-up before any wait)
   const int i0 = blockIdx.y * kTileI;
   if (i0 >= 3 && i0 + kTileI + 3 <= g.Nu)
-    hydro32p_tile<G2, FM, true>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum);
+    hydro32p_tile<G2, FM, true>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum, &tmS,
+                                &tmU, &tmW, &tmP, &bar_ld);
   else
-    hydro32p_tile<G2, FM, false>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum);
+    hydro32p_tile<G2, FM, false>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum, &tmS,
+                                 &tmU, &tmW, &tmP, &bar_ld);
 }
 
 }  // namespace dg

@@ -71,6 +71,8 @@ struct MixedState {
   // pipeline stages of each gravity product (slots: 0 phi DFT, 1-4 the u passes, 5 inverse
   // phi DFT; 0 = chosen by K) and the tuner's record (autotune below)
   int ns[6] = {0, 0, 0, 0, 0, 0};
+  // FP32 field tiles of the packed hydro kernel: sigma, u, w of both ping-pong buffers, dPhi
+  CUtensorMap mSig[2], mU[2], mW[2], mPhi;
   bool tuned = false;
   std::string tune_info;
   // A = 32 (Nu = 1024): the four u passes run as one fused kernel (uconv.cuh)
@@ -118,8 +120,8 @@ static cudaError_t hydro32t_prepare() {
                        (const void *)k_hydro32p<true, kForcePhi>, (const void *)k_hydro32p<false, kForcePhi>,
                        (const void *)k_hydro32p<true, kForceArrays>, (const void *)k_hydro32p<false, kForceArrays>,
                        (const void *)k_hydro32p<true, kForceNone>, (const void *)k_hydro32p<false, kForceNone>};
-  for (const void *f : fns) {
-    cudaError_t e = smem_attrs(f, kSmem32t);
+  for (int q = 0; q < 12; ++q) {
+    cudaError_t e = smem_attrs(fns[q], q < 6 ? kSmem32t : kSmem32p);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -131,6 +133,22 @@ static bool u_factored(int Nu) { return Nu % 1024 == 0; }
 static bool u_fused(int Nu) { return Nu == 1024; }
 // the forward phi transform as a fused two-stage kernel (phifwd.cuh) when both are 1024
 static bool phi_fused(int Nu, int Nphi) { return Nu == 1024 && Nphi == 1024; }
+
+// Row-major FP32 field [rows][cols] -> boxes of 64 columns x 22 rows, no swizzle (the
+// packed hydro kernel's input tile; rows outside the field read as zero).
+static bool make_map_f32(CUtensorMap *m, const void *base, uint64_t rows, uint64_t cols) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  if (((uintptr_t)base & 15) || (cols * 4) % 16) return false;
+  cuuint64_t gdim[2] = {cols, rows};
+  cuuint64_t gstride[1] = {cols * 4};
+  cuuint32_t box[2] = {(cuuint32_t)kLd32t, (cuuint32_t)kRows32t};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), gdim, gstride, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
 
 // K-major BF16 matrix [rows][cols] -> tiles of box_rows x 64 with 128-byte swizzle.
 static bool make_map(CUtensorMap *m, const void *base, uint64_t rows, uint64_t cols, uint32_t box_rows) {
@@ -645,7 +663,14 @@ int dg_handle::mixed_init() {
     if (hk && strcmp(hk, "warp") == 0) X.hydro_kind = MixedState::kHydroWarp;
     if (hk && strcmp(hk, "packed") == 0) X.hydro_kind = MixedState::kHydroPacked;
     if (Nphi < kLd32t || Nphi % 2) X.hydro_kind = MixedState::kHydroWarp;
-    if (X.hydro_kind != MixedState::kHydroWarp) XK(hydro32t_prepare());
+    if (X.hydro_kind != MixedState::kHydroWarp) {
+      XK(hydro32t_prepare());
+      bool okh = make_map_f32(&X.mPhi, X.dPhi, Nu, Nphi);
+      for (int b = 0; b < 2; ++b)
+        okh = okh && make_map_f32(&X.mSig[b], X.sig[b], Nu, Nphi) && make_map_f32(&X.mU[b], X.u[b], Nu, Nphi) &&
+              make_map_f32(&X.mW[b], X.w[b], Nu, Nphi);
+      if (!okh) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed (hydro tiles)");
+    }
   }
   X.tables_ready = true;
   return DG_OK;
@@ -997,8 +1022,10 @@ static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *
     dim3 grid((X.Nphi + kTileJp - 1) / kTileJp, (X.Nu + kTileI - 1) / kTileI);
     const SplitBf16 sx{X.Sx.hi, X.Sx.lo};
     cudaError_t e = cudaSuccess;
+    const int b = (sig == X.sig[1]) ? 1 : 0;  // which ping-pong buffer holds the input
     auto go = [&](auto kern) {
-      e = launch_pdl(kern, grid, dim3(kThreads32t), kSmem32t, st, sig, u, w, Phi, gR, gp, so, uo, wo, sx, ctl, X.rows);
+      e = launch_pdl(kern, grid, dim3(kThreads32t), kSmem32p, st, X.mSig[b], X.mU[b], X.mW[b], X.mPhi, sig, u, w, Phi,
+                     gR, gp, so, uo, wo, sx, ctl, X.rows);
     };
     const bool g2 = X.rows.gamma2 != 0;
     if (fm == kForcePhi) g2 ? go(k_hydro32p<true, kForcePhi>) : go(k_hydro32p<false, kForcePhi>);
