@@ -432,7 +432,7 @@ def main():
         tuned = disk.tuning()
         form = next((f for f in ("packed", "tile", "warp") if ("hydro " + f) in tuned), "tile")
         hyd_name = {
-            "packed": "fused hydro sweep (k_hydro32p: 16 x 56 tiles, TMA-staged fields, FP32x2 column pairs, "
+            "packed": "fused hydro sweep (k_hydro32p: 16 x 58 tiles, TMA-staged fields, FP32x2 column pairs, "
                       "source + R sweep + phi sweep + CFL)",
             "tile": "fused hydro sweep (k_hydro32t: 16 x 58 tiles, source + R sweep + phi sweep + CFL)",
             "warp": "fused hydro sweep (k_hydro32w: warp-marching rows, source + R sweep + phi sweep + CFL)",

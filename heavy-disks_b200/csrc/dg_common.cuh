@@ -65,6 +65,35 @@ __device__ __forceinline__ V cmul(V a, V b) {
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Row-tile hand-over from the hydro step to the forward phi transform of the next step.
+// The inverse phi transform (the hydro's predecessor) arms one counter per 16-row tile row
+// with the hydro launch's column-tile count.  Each hydro CTA, once all of its writes are
+// issued, decrements its row's counter with release semantics (rowtile_done).  A phi
+// transform CTA waits, with acquire semantics, until the counter of the rows it reads is
+// zero (rowtile_wait) instead of waiting for the whole hydro grid, so early rows are
+// transformed while the hydro's last CTAs still run.  The phi transform is launched with
+// programmatic dependence, i.e. only after every hydro CTA has started, so the counters
+// always reach zero; the wait is bounded all the same (~1 s of SM clock, then kStTimeout).
+__device__ __forceinline__ void rowtile_done(int *cnt) {
+  __syncthreads();  // every thread's stores precede the release below
+  if (threadIdx.x == 0) asm volatile("red.release.gpu.global.add.s32 [%0], -1;" ::"l"(cnt) : "memory");
+}
+__device__ __forceinline__ bool rowtile_wait(const int *cnt, int *status) {
+  if (status && *(volatile int *)status) return false;  // an earlier wait gave up: the step is void
+  long long start = 0;
+  for (uint32_t it = 0;; ++it) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(cnt) : "memory");
+    if (v <= 0) return true;
+    if (it == 64) start = clock64();
+    if (it > 64 && clock64() - start > (1ll << 31)) {
+      if (status) atomicOr(status, kStTimeout);
+      return false;
+    }
+    __nanosleep(128);
+  }
+}
+
 // Ordered atomic max for non-negative doubles (NaN compares above +inf, so a NaN
 // propagates into the max and is caught by the non-finite check).
 __device__ __forceinline__ void atomic_max_pos(unsigned long long *addr, double v) {

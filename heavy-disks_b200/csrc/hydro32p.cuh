@@ -3,18 +3,22 @@
 // in FP32x2 registers (Blackwell's paired FADD2 / FMUL2 / FFMA2), so one instruction, one
 // shared-memory access and one set of row constants serve two zones.
 //
-// Tile: kTileI rows x kTileJp = 56 output columns, stored columns c = j - (j0 - 4) in
-// [0, 64) (a 4-column halo on each side keeps every column pair, and every global pair
-// access, 8-byte aligned, also across the periodic wrap).  Lane l of a warp owns the pair
-// (2l, 2l+1) of every row it visits; warp w visits rows w, w + 8, ...  Azimuthal
-// neighbours (columns 2l - 2 .. 2l + 2) come from the neighbouring lanes by shuffle.
-// Columns whose results are never used (lanes 0 and 31 in the sweeps) are computed
-// anyway and discarded, so shuffles run with every lane active.
+// Tile: kTileI rows x kTileJp = 58 output columns.  Stored columns c in [0, 64) hold the
+// unwrapped columns J = j0 - 3 + c (a 3-column halo on each side); the outputs are
+// c in [3, 61).  Tile bx starts at j0 = 58 bx + 1, so j0 - 3 is even and every column
+// pair, and every global pair access, stays 8-byte aligned, also across the periodic
+// wrap; the tiles cover J = 1 .. Nphi, column Nphi being column 0.  Lane l of a warp owns
+// the pair (2l, 2l+1) of every row it visits (lanes 1 and 30 output one half); warp w
+// visits rows w, w + 8, ...  Azimuthal neighbours (columns 2l - 2 .. 2l + 2) come from the
+// neighbouring lanes by shuffle.  Columns whose results are never used are computed anyway
+// and discarded, so shuffles run with every lane active.  With 58 columns a 1024-column
+// grid takes 18 column tiles, so a 1024 x 1024 launch is 1152 CTAs: under two waves of
+// four CTAs on each of the 148 SMs.
 //
 // Interior column tiles (no periodic wrap inside the tile) with self-gravity or no force
-// stage sigma, u, w and dPhi in shared memory as one TMA box each (64 x 22 floats, rows
-// outside the grid read as zero); the two edge tiles and the caller-forces path use
-// thread loads.
+// stage sigma, u, w and dPhi in shared memory as one TMA box each (68 x 22 floats from the
+// 16-byte-aligned column at or left of j0 - 3; rows outside the grid read as zero); the
+// two edge tiles and the caller-forces path use thread loads.
 #pragma once
 
 #include "hydro32t.cuh"
@@ -22,7 +26,8 @@
 
 namespace dg {
 
-constexpr int kTileJp = kLd32t - 8;        // output columns per CTA (56)
+constexpr int kTileJp = kLd32t - 6;        // output columns per CTA (58)
+constexpr int kLdP = kLd32t + 4;           // floats per staged row: a TMA box from the aligned column
 constexpr int kWarps32p = kThreads32t / 32;  // 8 row groups, one warp each
 constexpr int kItLoadP = (kRows32t + kWarps32p - 1) / kWarps32p;
 constexpr int kItSrcP = (kSrcRows32t + kWarps32p - 1) / kWarps32p;
@@ -30,11 +35,16 @@ constexpr int kItFaceP = (kFaceRows32t + kWarps32p - 1) / kWarps32p;
 constexpr int kItOutP = (kTileI + kWarps32p - 1) / kWarps32p;
 static_assert(kItOutP * kWarps32p == kTileI, "output rows split evenly over the warps");
 // shared-memory plan of this kernel in floats: the five staged fields first (each one TMA
-// box, 16-byte aligned), then the radial fluxes and the row constants.  u1 / w1 (source rows
-// i0-2 ..) overwrite the raw u / w of the same points one row down, in place.
-constexpr int kFieldP = kRows32t * kLd32t;  // 22 x 64
-constexpr int kOffSgP = 0, kOffDpP = kFieldP, kOffPhP = 2 * kFieldP, kOffU0P = 3 * kFieldP, kOffW0P = 4 * kFieldP;
-constexpr int kOffFP = 5 * kFieldP;
+// box of kRows32t x kLdP; a TMA destination in shared memory is 128-byte aligned, so each
+// field is padded to a multiple of 32 floats), then the radial fluxes and the row
+// constants.  u1 / w1 (source rows i0-2 ..) overwrite the raw u / w of the same points one
+// row down, in place.
+constexpr int kFieldP = kRows32t * kLdP;            // 22 x 68 floats of one box
+constexpr int kFieldStrideP = (kFieldP + 31) / 32 * 32;  // 1504
+constexpr int kOffSgP = 0, kOffDpP = kFieldStrideP, kOffPhP = 2 * kFieldStrideP, kOffU0P = 3 * kFieldStrideP,
+              kOffW0P = 4 * kFieldStrideP;
+static_assert(kOffPhP % 32 == 0 && kOffU0P % 32 == 0 && kOffW0P % 32 == 0, "TMA destinations 128-byte aligned");
+constexpr int kOffFP = 5 * kFieldStrideP;
 constexpr int kOffRcP = kOffFP + 4 * kFaceArr32t;
 constexpr size_t kSmem32p = (size_t)(kOffRcP + tNConst * kRows32t) * sizeof(float) + 128;  // + alignment slack
 constexpr uint32_t kFieldBytesP = kFieldP * 4;
@@ -71,11 +81,19 @@ __device__ __forceinline__ void hydro32p_tile(
     const CUtensorMap *tmU, const CUtensorMap *tmW, const CUtensorMap *tmP, uint64_t *bar_ld) {
   using namespace p2;
   float *rc = sm32t + kOffRcP;
-  // shared arrays as pairs: row r, lane l -> element r * 32 + l
-  constexpr int L2 = kLd32t / 2;
-  F2 *SG = reinterpret_cast<F2 *>(sm32t + kOffSgP), *DP = reinterpret_cast<F2 *>(sm32t + kOffDpP);
-  F2 *PH = reinterpret_cast<F2 *>(sm32t + kOffPhP);
-  F2 *U0 = reinterpret_cast<F2 *>(sm32t + kOffU0P), *W0 = reinterpret_cast<F2 *>(sm32t + kOffW0P);
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  const int Nu = g.Nu, Nphi = g.Nphi;
+  const int i0 = blockIdx.y * kTileI, j0 = blockIdx.x * kTileJp + 1;
+  const int ib = i0 - 3;
+  // staged fields as pairs: row r, lane l -> element r * L2 + l (+ po).  A TMA box starts at
+  // the 16-byte-aligned column xa = j0 - 3 - 2 po, po = 0 or 1 (j0 - 3 is even)
+  const int xs0 = j0 - 3;
+  const bool use_tma = FM != kForceArrays && xs0 >= 0 && xs0 + kLd32t <= Nphi;  // CTA-uniform
+  const int po = use_tma ? (xs0 & 3) >> 1 : 0;
+  constexpr int L2 = kLdP / 2, LF = kLd32t / 2;  // pair strides: staged fields, face arrays
+  F2 *SG = reinterpret_cast<F2 *>(sm32t + kOffSgP) + po, *DP = reinterpret_cast<F2 *>(sm32t + kOffDpP) + po;
+  F2 *PH = reinterpret_cast<F2 *>(sm32t + kOffPhP) + po;
+  F2 *U0 = reinterpret_cast<F2 *>(sm32t + kOffU0P) + po, *W0 = reinterpret_cast<F2 *>(sm32t + kOffW0P) + po;
   F2 *U1 = U0 + L2, *W1 = W0 + L2;  // source row rs = stored row rs + 1
   F2 *FF = reinterpret_cast<F2 *>(sm32t + kOffFP), *FR = FF + kFaceArr32t / 2, *GA = FR + kFaceArr32t / 2,
      *GB = GA + kFaceArr32t / 2;
@@ -83,15 +101,11 @@ __device__ __forceinline__ void hydro32p_tile(
   F2 *PF = FF, *PR = FR, *PG = GA;  // S5 outputs over the dead radial fluxes
   F2 *S3 = U1;                      // new sigma for the mode sums
 
-  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-  const int Nu = g.Nu, Nphi = g.Nphi;
-  const int i0 = blockIdx.y * kTileI, j0 = blockIdx.x * kTileJp;
-  const int ib = i0 - 3;
   const int iend = (i0 + kTileI < Nu) ? i0 + kTileI : Nu;
-  const int jc = wrap_col(j0 - 4 + 2 * lane, Nphi);  // global column of this lane's first element (even)
-  // output columns c in [4, 60): lanes 2..29, each element inside the grid
-  const bool out_lane = lane >= 2 && lane < 2 + kTileJp / 2;
-  const bool outx = out_lane && j0 + 2 * lane - 4 < Nphi, outy = out_lane && j0 + 2 * lane - 3 < Nphi;
+  const int jc = wrap_col(xs0 + 2 * lane, Nphi);  // global column of this lane's first element (even)
+  // output columns c in [3, 61) with J = xs0 + c <= Nphi: .x on lanes 2..30, .y on lanes 1..29
+  const bool outx = lane >= 2 && lane <= 30 && xs0 + 2 * lane <= Nphi;
+  const bool outy = lane >= 1 && lane <= 29 && xs0 + 2 * lane + 1 <= Nphi;
 #define RC(k, i) rc[(k) * kRows32t + (i) - ib]
   auto row_ok = [&](int i) { return IN || (i >= 0 && i < Nu); };
   auto first_row = [&](int i) { return !IN && i == 0; };
@@ -159,14 +173,14 @@ __device__ __forceinline__ void hydro32p_tile(
   }
 
   // ---- S0: sigma, u, w, dPhi of rows i0-3 .. i0+kTileI+2 into shared memory ----
-  const bool use_tma = FM != kForceArrays && j0 >= 4 && j0 - 4 + kLd32t <= Nphi;  // CTA-uniform
   if (use_tma) {
     if (tid == 0) {
+      const int xa = xs0 - 2 * po;  // a multiple of 4 columns (16 bytes)
       tc::mbar_arrive_expect_tx(bar_ld, (FM == kForcePhi ? 4u : 3u) * kFieldBytesP);
-      tc::tma_load_2d(sm32t + kOffSgP, tmS, bar_ld, j0 - 4, ib);
-      tc::tma_load_2d(sm32t + kOffU0P, tmU, bar_ld, j0 - 4, ib);
-      tc::tma_load_2d(sm32t + kOffW0P, tmW, bar_ld, j0 - 4, ib);
-      if (FM == kForcePhi) tc::tma_load_2d(sm32t + kOffPhP, tmP, bar_ld, j0 - 4, ib);
+      tc::tma_load_2d(sm32t + kOffSgP, tmS, bar_ld, xa, ib);
+      tc::tma_load_2d(sm32t + kOffU0P, tmU, bar_ld, xa, ib);
+      tc::tma_load_2d(sm32t + kOffW0P, tmW, bar_ld, xa, ib);
+      if (FM == kForcePhi) tc::tma_load_2d(sm32t + kOffPhP, tmP, bar_ld, xa, ib);
     }
   } else {
     F2 sv[kItLoadP], pv[kItLoadP], uv[kItLoadP], wv[kItLoadP];
@@ -315,7 +329,7 @@ __device__ __forceinline__ void hydro32p_tile(
         GAv = mul(F, Df);
         GBv = mul(F, sub(Df, S(dVf)));
       }
-      const int x = fr * L2 + lane;
+      const int x = fr * LF + lane;
       FF[x] = F; FR[x] = FRv; GA[x] = GAv; GB[x] = GBv;
     }
   }
@@ -326,15 +340,15 @@ __device__ __forceinline__ void hydro32p_tile(
   for (int k = 0; k < kItOutP; ++k) {
     const int ri = wp + kWarps32p * k, i = i0 + ri;
     if (IN || i < iend) {
-      const int xs = (i - ib) * L2 + lane, xu = (i - ib - 1) * L2 + lane, xf = ri * L2 + lane;
+      const int xs = (i - ib) * L2 + lane, xu = (i - ib - 1) * L2 + lane, xf = ri * LF + lane;
       const F2 sgi = SG[xs], u1i = U1[xu], w1i = W1[xu];
       const float S0 = RC(tS0, i), iv = RC(tInvVol, i);
       const F2 s = add(S(S0), sgi);
-      const F2 s2 = fma(mul(S(dt), sub(FF[xf], FF[xf + L2])), S(iv), sgi);
+      const F2 s2 = fma(mul(S(dt), sub(FF[xf], FF[xf + LF])), S(iv), sgi);
       const F2 sn = add(S(S0), s2);
       const F2 d = make_float2(sn.x < 1e-10f ? 1e-10f : sn.x, sn.y < 1e-10f ? 1e-10f : sn.y);
-      const F2 u2 = fdiv(fma(mul(S(dt), sub(FR[xf], FR[xf + L2])), S(iv), mul(s, u1i)), d);
-      const F2 w2 = fdiv(fma(mul(S(dt), sub(GB[xf], GA[xf + L2])), S(iv), mul(s, w1i)), d);
+      const F2 u2 = fdiv(fma(mul(S(dt), sub(FR[xf], FR[xf + LF])), S(iv), mul(s, u1i)), d);
+      const F2 w2 = fdiv(fma(mul(S(dt), sub(GB[xf], GA[xf + LF])), S(iv), mul(s, w1i)), d);
       SG[xs] = s2;
       U2[xs] = u2;
       W2[xs] = w2;
@@ -372,7 +386,7 @@ __device__ __forceinline__ void hydro32p_tile(
       const F2 uf = fma(hf, vanleer(sub(uc, ub), sub(ub, ua)), ub);
       const F2 wf = fma(hf, vanleer(sub(wc, wb), sub(wb, wa)), wb);
       const F2 Ffull = mul(mul(vf, Sf), S(A));
-      const int xf = ri * L2 + lane;
+      const int xf = ri * LF + lane;
       PF[xf] = mul(S(A), fma(S(V), sf, mul(dv, Sf)));
       PR[xf] = mul(Ffull, uf);
       PG[xf] = mul(Ffull, wf);
@@ -385,7 +399,7 @@ __device__ __forceinline__ void hydro32p_tile(
   for (int k = 0; k < kItOutP; ++k) {
     const int ri = wp + kWarps32p * k, i = i0 + ri;
     if (IN || i < iend) {
-      const int x = (i - ib) * L2 + lane, xf = ri * L2 + lane;
+      const int x = (i - ib) * L2 + lane, xf = ri * LF + lane;
       const F2 fm = PF[xf], fr = PR[xf], fg = PG[xf];
       // right face of column 2l+1 is the right lane's first face
       const F2 fm1 = make_float2(fm.y, dn1(fm.x)), fr1 = make_float2(fr.y, dn1(fr.x)), fg1 = make_float2(fg.y, dn1(fg.x));
@@ -412,10 +426,14 @@ __device__ __forceinline__ void hydro32p_tile(
           *reinterpret_cast<F2 *>(wo + q) = w3;
           *reinterpret_cast<__nv_bfloat162 *>(Sx.hi + q) = __halves2bfloat162(hx, hy);
           *reinterpret_cast<__nv_bfloat162 *>(Sx.lo + q) = __halves2bfloat162(lx, ly);
-        } else {  // the last tile's edge: one element inside the grid
+        } else if (outx) {  // one half of the pair is output (tile edges)
           so[q] = s3.x; uo[q] = u3.x; wo[q] = w3.x;
           Sx.hi[q] = hx;
           Sx.lo[q] = lx;
+        } else {
+          so[q + 1] = s3.y; uo[q + 1] = u3.y; wo[q + 1] = w3.y;
+          Sx.hi[q + 1] = hy;
+          Sx.lo[q + 1] = ly;
         }
         // CFL rate of the new state (hydro.hpp:54-57)
         const F2 scl = make_float2(flx ? 1e-10f : sn3.x, fly ? 1e-10f : sn3.y);
@@ -487,7 +505,8 @@ __global__ void __launch_bounds__(kThreads32t, 4) k_hydro32p(
     const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUtensorMap tmP,
     const float *__restrict__ sig, const float *__restrict__ uu, const float *__restrict__ ww,
     const float *__restrict__ Phi, const double *__restrict__ gRin, const double *__restrict__ gpin,
-    float *__restrict__ so, float *__restrict__ uo, float *__restrict__ wo, SplitBf16 Sx, Ctl *ctl, Rows32 g) {
+    float *__restrict__ so, float *__restrict__ uo, float *__restrict__ wo, SplitBf16 Sx, Ctl *ctl, Rows32 g,
+    int *rowpend) {
   extern __shared__ __align__(16) uint8_t sm32p_raw[];
   // TMA destinations: the field offsets are multiples of 128 bytes from a 128-aligned base
   float *sm32t = reinterpret_cast<float *>(((uintptr_t)sm32p_raw + 127) & ~(uintptr_t)127);
@@ -506,6 +525,7 @@ __global__ void __launch_bounds__(kThreads32t, 4) k_hydro32p(
   else
     hydro32p_tile<G2, FM, false>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum, &tmS,
                                  &tmU, &tmW, &tmP, &bar_ld);
+  if (rowpend) rowtile_done(rowpend + blockIdx.y);  // this tile's outputs are written
 }
 
 }  // namespace dg

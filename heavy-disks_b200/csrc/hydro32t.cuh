@@ -387,7 +387,8 @@ template <bool G2, int FM>
 __global__ void __launch_bounds__(kThreads32t, 4) k_hydro32t(
     const float *__restrict__ sig, const float *__restrict__ uu, const float *__restrict__ ww,
     const float *__restrict__ Phi, const double *__restrict__ gRin, const double *__restrict__ gpin,
-    float *__restrict__ so, float *__restrict__ uo, float *__restrict__ wo, SplitBf16 Sx, Ctl *ctl, Rows32 g) {
+    float *__restrict__ so, float *__restrict__ uo, float *__restrict__ wo, SplitBf16 Sx, Ctl *ctl, Rows32 g,
+    int *rowpend) {
   extern __shared__ float sm32t[];
   __shared__ double red[kThreads32t / 32];
   __shared__ double bsum[2 * kMaxModes], zsum[2 * kMaxModes];
@@ -396,6 +397,7 @@ __global__ void __launch_bounds__(kThreads32t, 4) k_hydro32t(
     hydro32t_tile<G2, FM, true>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum);
   else
     hydro32t_tile<G2, FM, false>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum);
+  if (rowpend) rowtile_done(rowpend + blockIdx.y);  // this tile's outputs are written
 }
 
 }  // namespace dg

@@ -73,6 +73,15 @@ struct MixedState {
   int ns[6] = {0, 0, 0, 0, 0, 0};
   // FP32 field tiles of the packed hydro kernel: sigma, u, w of both ping-pong buffers, dPhi
   CUtensorMap mSig[2], mU[2], mW[2], mPhi;
+  // row-tile counters between a step's hydro kernel and the next step's fused phi transform
+  // (dg_common.cuh rowtile_*); zero between steps.  rs_step: the gravity being enqueued is
+  // part of a time step whose hydro signals them.  DISKGPU_ROWSYNC=0 turns the hand-over off
+  // (the phi transform then waits for the whole hydro grid).
+  int *rowpend = nullptr;
+  bool rs_step = false, rowsync = true;
+  bool rowsync_ok() const {
+    return rowsync && fused_phi && rowpend && (hydro_kind == kHydroTile || hydro_kind == kHydroPacked);
+  }
   bool tuned = false;
   std::string tune_info;
   // A = 32 (Nu = 1024): the four u passes run as one fused kernel (uconv.cuh)
@@ -134,7 +143,7 @@ static bool u_fused(int Nu) { return Nu == 1024; }
 // the forward phi transform as a fused two-stage kernel (phifwd.cuh) when both are 1024
 static bool phi_fused(int Nu, int Nphi) { return Nu == 1024 && Nphi == 1024; }
 
-// Row-major FP32 field [rows][cols] -> boxes of 64 columns x 22 rows, no swizzle (the
+// Row-major FP32 field [rows][cols] -> boxes of 68 columns x 22 rows, no swizzle (the
 // packed hydro kernel's input tile; rows outside the field read as zero).
 static bool make_map_f32(CUtensorMap *m, const void *base, uint64_t rows, uint64_t cols) {
   auto fn = encode_fn();
@@ -142,7 +151,7 @@ static bool make_map_f32(CUtensorMap *m, const void *base, uint64_t rows, uint64
   if (((uintptr_t)base & 15) || (cols * 4) % 16) return false;
   cuuint64_t gdim[2] = {cols, rows};
   cuuint64_t gstride[1] = {cols * 4};
-  cuuint32_t box[2] = {(cuuint32_t)kLd32t, (cuuint32_t)kRows32t};
+  cuuint32_t box[2] = {(cuuint32_t)kLdP, (cuuint32_t)kRows32t};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), gdim, gstride, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -565,6 +574,13 @@ int dg_handle::mixed_init() {
   XK(alloc_split(X.Cu, (size_t)2 * Nu * Nu)); XK(alloc_split(X.CuT, (size_t)2 * Nu * Nu));
   XK(dalloc(&X.KW, (size_t)Nphi * 2 * Nu));
   XK(dalloc(&X.dPhi, n));
+  static_assert(kTileI == tc::kPfHydroRows && kTileI % tc::kPfRows == 0, "row tiles of the hand-over");
+  XK(dalloc(&X.rowpend, (size_t)(Nu + kTileI - 1) / kTileI));
+  {
+    const char *rs = getenv("DISKGPU_ROWSYNC");
+    X.rowsync = !(rs && strcmp(rs, "0") == 0);
+  }
+  XK(cudaMemsetAsync(X.rowpend, 0, (size_t)(Nu + kTileI - 1) / kTileI * sizeof(int), st));
   XK(dalloc(&X.phiscale, Nu));
   XK(dalloc(&X.rowbuf, (size_t)24 * (Nu + 1)));
   XK(dalloc(&X.rowbufd, (size_t)4 * Nu));
@@ -697,7 +713,7 @@ void dg_handle::mixed_release() {
   SplitBuf *bufs[] = {&X.Sx, &X.X1, &X.Wt, &X.Z, &X.Fphi, &X.Cu, &X.CuT, &X.Gphi,
                       &X.Xin, &X.Tb, &X.Yk, &X.Ub, &X.RB, &X.RA, &X.RGA, &X.RGB, &X.PA, &X.PB};
   for (SplitBuf *b : bufs) free_split(*b);
-  void *ptrs[] = {X.KW, X.dPhi, X.phiscale, X.rowbuf, X.rowbufd, X.KW2, X.tw, X.khm, X.twp, X.twphi};
+  void *ptrs[] = {X.KW, X.dPhi, X.rowpend, X.phiscale, X.rowbuf, X.rowbufd, X.KW2, X.tw, X.khm, X.twp, X.twphi};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   delete mx;
@@ -815,7 +831,7 @@ static int build_basic(dg_handle *h, const double *Sig, const double *vp) {
 
 static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *u, const float *w, const float *Phi,
                                   const double *gR, const double *gp, int fm, float *so, float *uo, float *wo, Ctl *ctl,
-                                  cudaStream_t st);
+                                  cudaStream_t st, int *rowpend = nullptr);
 
 int dg_handle::mixed_upload_state(const double *Sig, const double *vRh, const double *vph) {
   MixedState &X = *mx;
@@ -830,6 +846,8 @@ int dg_handle::mixed_upload_state(const double *Sig, const double *vRh, const do
   XK(cudaMemcpyAsync(VP[0], vph, n * sizeof(double), cudaMemcpyHostToDevice, st));
   k_to_pert<<<grid_for(n), 256, 0, st>>>(S[0], VR[0], VP[0], X.sig[cur], X.u[cur], X.w[cur], X.Sx, X.rows);
   XK(cudaGetLastError());
+  // no hydro step is in flight: the row-tile counters start from zero
+  XK(cudaMemsetAsync(X.rowpend, 0, (size_t)(p.Nu + kTileI - 1) / kTileI * sizeof(int), st));
   if (!in_step_host && !X.tuned) {
     int rc = mixed_autotune();
     if (rc) return rc;
@@ -1017,7 +1035,7 @@ int dg_handle::mixed_download_state(double *Sig, double *vRh, double *vph) {
 
 static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *u, const float *w, const float *Phi,
                                   const double *gR, const double *gp, int fm, float *so, float *uo, float *wo, Ctl *ctl,
-                                  cudaStream_t st) {
+                                  cudaStream_t st, int *rowpend) {
   if (X.hydro_kind == MixedState::kHydroPacked) {
     dim3 grid((X.Nphi + kTileJp - 1) / kTileJp, (X.Nu + kTileI - 1) / kTileI);
     const SplitBf16 sx{X.Sx.hi, X.Sx.lo};
@@ -1025,7 +1043,7 @@ static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *
     const int b = (sig == X.sig[1]) ? 1 : 0;  // which ping-pong buffer holds the input
     auto go = [&](auto kern) {
       e = launch_pdl(kern, grid, dim3(kThreads32t), kSmem32p, st, X.mSig[b], X.mU[b], X.mW[b], X.mPhi, sig, u, w, Phi,
-                     gR, gp, so, uo, wo, sx, ctl, X.rows);
+                     gR, gp, so, uo, wo, sx, ctl, X.rows, rowpend);
     };
     const bool g2 = X.rows.gamma2 != 0;
     if (fm == kForcePhi) g2 ? go(k_hydro32p<true, kForcePhi>) : go(k_hydro32p<false, kForcePhi>);
@@ -1038,7 +1056,8 @@ static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *
     const SplitBf16 sx{X.Sx.hi, X.Sx.lo};
     cudaError_t e = cudaSuccess;
     auto go = [&](auto kern) {
-      e = launch_pdl(kern, grid, dim3(kThreads32t), kSmem32t, st, sig, u, w, Phi, gR, gp, so, uo, wo, sx, ctl, X.rows);
+      e = launch_pdl(kern, grid, dim3(kThreads32t), kSmem32t, st, sig, u, w, Phi, gR, gp, so, uo, wo, sx, ctl, X.rows,
+                     rowpend);
     };
     const bool g2 = X.rows.gamma2 != 0;
     if (fm == kForcePhi) g2 ? go(k_hydro32t<true, kForcePhi>) : go(k_hydro32t<false, kForcePhi>);
@@ -1046,6 +1065,7 @@ static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *
     else g2 ? go(k_hydro32t<true, kForceNone>) : go(k_hydro32t<false, kForceNone>);
     return e;
   }
+  if (rowpend) return cudaErrorInvalidValue;  // the warp form has no row-tile hand-over
   const int nstrips = (X.Nphi + kOutCols32 - 1) / kOutCols32;
   dim3 grid((nstrips + kWarps32 - 1) / kWarps32, (X.Nu + kBand32 - 1) / kBand32);
   k_hydro32w<<<grid, kWarps32 * 32, 0, st>>>(sig, u, w, Phi, gR, gp, fm, so, uo, wo, SplitBf16{X.Sx.hi, X.Sx.lo}, ctl,
@@ -1068,7 +1088,8 @@ int dg_handle::mixed_gravity() {
     XK(prof_begin(DG_PROF_GRAV_PHI_FWD));
     if (X.fused_phi) {
       // real 32-point stage, twiddle, complex 32-point stage: 4 rows per CTA
-      tc::PhiFwdArgs f{X.Sx.hi, X.Sx.lo, X.twphi, X.Xin.hi, X.Xin.lo, nm * A, Nphi, &ctl->status};
+      tc::PhiFwdArgs f{X.Sx.hi, X.Sx.lo, X.twphi, X.Xin.hi, X.Xin.lo, nm * A, Nphi, &ctl->status,
+                       X.rs_step ? X.rowpend : nullptr};
       XK(launch_pdl(tc::k_phifwd, dim3(Nu / tc::kPfRows), dim3(tc::kPfThreads), tc::kPfSmem, st, X.mPA[0], X.mPA[1],
                     X.mPB[0], X.mPB[1], f));
     } else {
@@ -1098,8 +1119,14 @@ int dg_handle::mixed_gravity() {
       XK(gemm<tc::kEpiI2ToZ>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st, X.ns[4]));
     }
     XK(prof_end(DG_PROF_GRAV_U));
-    // G4: inverse phi DFT with Z as an MN-major operand
+    // G4: inverse phi DFT with Z as an MN-major operand; in a time step it arms the hydro's
+    // row-tile counters with the hydro launch's column-tile count
     a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi; a.row_scale = X.phiscale;
+    if (X.rs_step) {
+      a.rowpend = X.rowpend;
+      a.rp_n = (Nu + kTileI - 1) / kTileI;
+      a.rp_val = X.hydro_kind == MixedState::kHydroPacked ? (Nphi + kTileJp - 1) / kTileJp : (Nphi + kTileJ - 1) / kTileJ;
+    }
     XK(prof_begin(DG_PROF_GRAV_PHI_INV));
     XK((gemm<tc::kEpiRowScaleF32, true, false>(X.mZmn[0], X.mZmn[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st,
                                                X.ns[5])));
@@ -1136,15 +1163,21 @@ int dg_handle::mixed_enqueue_step() {
   MixedState &X = *mx;
   const int c = cur, o = cur ^ 1;
   int fm = kForceNone;
+  // row-tile hand-over: this step's phi transform waits for the previous step's hydro rows,
+  // its inverse phi transform arms the counters this step's hydro counts down
+  const bool rs = p.selfgrav && X.rowsync_ok();
   if (p.selfgrav) {
     XK(prof_begin(DG_PROF_GRAVITY));
+    X.rs_step = rs;
     int rc = mixed_gravity();
+    X.rs_step = false;
     if (rc) return rc;
     XK(prof_end(DG_PROF_GRAVITY));
     fm = kForcePhi;
   }
   XK(prof_begin(DG_PROF_HYDRO));
-  XK(launch_hydro32(X, X.sig[c], X.u[c], X.w[c], X.dPhi, nullptr, nullptr, fm, X.sig[o], X.u[o], X.w[o], ctl, st));
+  XK(launch_hydro32(X, X.sig[c], X.u[c], X.w[c], X.dPhi, nullptr, nullptr, fm, X.sig[o], X.u[o], X.w[o], ctl, st,
+                    rs ? X.rowpend : nullptr));
   XK(prof_end(DG_PROF_HYDRO));
   cur = o;
   return DG_OK;

@@ -26,6 +26,7 @@ namespace dg {
 namespace tc {
 
 constexpr int kPfRows = 4;        // radial rows per CTA
+constexpr int kPfHydroRows = 16;  // rows of a hydro tile (the unit of the row-tile counters)
 constexpr int kPfThreads = 256;
 constexpr uint32_t kPfC = 0;      // stage-A operand C, 64 rows (m2, ro) x 64 K (j2 < 32 used) hi|lo 16 KB
 constexpr uint32_t kPfX = 16384;  // x slice, MN-major: 2 chunks of 32 K rows x 128 B          hi|lo 16 KB
@@ -41,6 +42,9 @@ struct PhiFwdArgs {
   int ld;                 // nmodes * 32
   int Nphi;
   int *status;
+  // hydro row-tile counters (dg_common.cuh rowtile_*): when set, this CTA waits for the
+  // 16-row tile row holding its rows instead of for the whole previous kernel
+  const int *rowpend;
 };
 
 __global__ void __launch_bounds__(kPfThreads, 2)
@@ -82,7 +86,14 @@ __global__ void __launch_bounds__(kPfThreads, 2)
     tma_load_2d(sm + kPfB, &tBh, &bar_in, 0, 0);
     tma_load_2d(sm + kPfB + 8192, &tBl, &bar_in, 0, 0);
   }
-  pdl_wait();  // the source comes from the previous kernel (and Xin's last reader is done)
+  // the source comes from the hydro step before this kernel (Xin's last reader, the u
+  // convolution of the previous step, completed before that hydro step started)
+  if (a.rowpend) {
+    if (threadIdx.x == 0) rowtile_wait(a.rowpend + i0 / kPfHydroRows, a.status);
+    __syncthreads();
+  } else {
+    pdl_wait();
+  }
   pdl_trigger();
   // x slice: chunk t of a plane = row pair ip, K row j2, 16-byte chunk c of the 128-byte row,
   // holding x[i0 + 2 ip + c / 4][32 j2 + 8 (c % 4) .. + 7]
@@ -92,7 +103,7 @@ __global__ void __launch_bounds__(kPfThreads, 2)
     for (int r = 0; r < 4; ++r) {
       const int t = threadIdx.x + kPfThreads * (r & 1), ip = t >> 8, j2 = (t >> 3) & 31, c = t & 7;
       const size_t g = (size_t)(i0 + 2 * ip + (c >> 2)) * a.Nphi + 32 * j2 + 8 * (c & 3);
-      xv[r] = *reinterpret_cast<const uint4 *>((r < 2 ? a.sx_hi : a.sx_lo) + g);
+      xv[r] = __ldcg(reinterpret_cast<const uint4 *>((r < 2 ? a.sx_hi : a.sx_lo) + g));  // L2: fresh after the wait
     }
 #pragma unroll
     for (int r = 0; r < 4; ++r) {

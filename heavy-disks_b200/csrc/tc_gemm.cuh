@@ -56,6 +56,10 @@ struct GemmArgs {
   // factored u-direction: A = i1 range (Nu / 32), Nphi, padded complex-mode count
   int fa, nphi, nmodes;
   const float2 *twiddle;  // W_M^{p2 i1}, [64][fa]
+  // row-tile counters of the hydro step that follows (dg_common.cuh rowtile_*): CTA (0, 0)
+  // sets rowpend[0 .. rp_n) = rp_val once this kernel's predecessor has completed
+  int *rowpend;
+  int rp_n, rp_val;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -299,6 +303,8 @@ __global__ void __launch_bounds__(kThreads, (NS == 1 ? 4 : (NS == 2 ? 2 : 1)))
   const uint32_t tmem_d = tmem_slot;
   pdl_wait();  // operands come from the previous kernel on the stream
   pdl_trigger();
+  if (args.rowpend && blockIdx.x == 0 && blockIdx.y == 0)
+    for (int r = threadIdx.x; r < args.rp_n; r += blockDim.x) args.rowpend[r] = args.rp_val;
 
   if (warp == 0 && lane == 0) {
     // ---- TMA producer ----
