@@ -146,12 +146,23 @@ __device__ __forceinline__ void hydro32p_tile(
   }
   pdl_wait();  // dt, the state and dPhi come from earlier kernels on the stream
   pdl_trigger();
+  // ---- S0 (interior column tiles): sigma, u, w, dPhi of rows i0-3 .. i0+kTileI+2 by TMA,
+  // issued before the step info is read so that the two latencies overlap ----
+  if (use_tma && tid == 0) {
+    const int xa = xs0 - 2 * po;  // a multiple of 4 columns (16 bytes)
+    tc::mbar_arrive_expect_tx(bar_ld, (FM == kForcePhi ? 4u : 3u) * kFieldBytesP);
+    tc::tma_load_2d(sm32t + kOffSgP, tmS, bar_ld, xa, ib);
+    tc::tma_load_2d(sm32t + kOffU0P, tmU, bar_ld, xa, ib);
+    tc::tma_load_2d(sm32t + kOffW0P, tmW, bar_ld, xa, ib);
+    if (FM == kForcePhi) tc::tma_load_2d(sm32t + kOffPhP, tmP, bar_ld, xa, ib);
+  }
   const StepInfo si = read_step_info(ctl, true);
   const float dt = (float)si.dt;
   float lmaxf = 0.f;
   bool bad = false;
 
   if (!si.active) {
+    if (use_tma && tid == 0) tc::mbar_wait(bar_ld, 0, &ctl->status);  // no copy in flight at exit
     // pass-through: copy the tile and report the CFL rate of the unchanged state
 #pragma unroll
     for (int k = 0; k < kItOutP; ++k) {
@@ -172,17 +183,8 @@ __device__ __forceinline__ void hydro32p_tile(
     return;
   }
 
-  // ---- S0: sigma, u, w, dPhi of rows i0-3 .. i0+kTileI+2 into shared memory ----
-  if (use_tma) {
-    if (tid == 0) {
-      const int xa = xs0 - 2 * po;  // a multiple of 4 columns (16 bytes)
-      tc::mbar_arrive_expect_tx(bar_ld, (FM == kForcePhi ? 4u : 3u) * kFieldBytesP);
-      tc::tma_load_2d(sm32t + kOffSgP, tmS, bar_ld, xa, ib);
-      tc::tma_load_2d(sm32t + kOffU0P, tmU, bar_ld, xa, ib);
-      tc::tma_load_2d(sm32t + kOffW0P, tmW, bar_ld, xa, ib);
-      if (FM == kForcePhi) tc::tma_load_2d(sm32t + kOffPhP, tmP, bar_ld, xa, ib);
-    }
-  } else {
+  // ---- S0 (edge tiles, caller forces): the same rows by thread loads ----
+  if (!use_tma) {
     F2 sv[kItLoadP], pv[kItLoadP], uv[kItLoadP], wv[kItLoadP];
 #pragma unroll
     for (int k = 0; k < kItLoadP; ++k) {

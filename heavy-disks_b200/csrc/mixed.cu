@@ -901,13 +901,26 @@ int dg_handle::mixed_autotune() {
   const char *hk = getenv("DISKGPU_HYDRO32");
   // the warp form is the only one for odd or narrow grids; a user's choice stands
   const bool hydro_fixed = (hk && *hk) || X.hydro_kind == MixedState::kHydroWarp;
+  // DISKGPU_STAGES=s0,s1,s2,s3,s4,s5 fixes the pipeline depth of every gravity product
+  // (0 = chosen by K, else 1, 2 or 4) and skips their tuning
+  bool stages_fixed = false;
+  if (const char *sv = getenv("DISKGPU_STAGES")) {
+    int v[6], n = sscanf(sv, "%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]);
+    if (n != 6) return fail(DG_ERR_INVALID, "autotune", "DISKGPU_STAGES wants six comma-separated depths");
+    for (int k = 0; k < 6; ++k) {
+      if (v[k] != 0 && v[k] != 1 && v[k] != 2 && v[k] != 4)
+        return fail(DG_ERR_INVALID, "autotune", "DISKGPU_STAGES: a depth is 0, 1, 2 or 4");
+      X.ns[k] = v[k];
+    }
+    stages_fixed = true;
+  }
   const TuneKey key{p.Nu, p.Nphi, X.rows.gamma2, p.selfgrav};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
       if (!hydro_fixed) X.hydro_kind = it->second.hydro_kind;
-      memcpy(X.ns, it->second.ns, sizeof(X.ns));
+      if (!stages_fixed) memcpy(X.ns, it->second.ns, sizeof(X.ns));
       X.tune_info = it->second.info + " (cached)";
       return DG_OK;
     }
@@ -938,7 +951,13 @@ int dg_handle::mixed_autotune() {
     return cudaSuccess;
   };
   do {
-    if (p.selfgrav) {
+    if (p.selfgrav && stages_fixed) {
+      info += "gravity stages fixed";
+      for (int k = 0; k < 6; ++k) {
+        snprintf(buf, sizeof buf, " %d", X.ns[k]);
+        info += buf;
+      }
+    } else if (p.selfgrav) {
       const std::vector<int> slots = !X.factored ? std::vector<int>{0, 1, 2, 5}
                                      : (X.fused_u ? std::vector<int>{0, 5} : std::vector<int>{0, 1, 2, 3, 4, 5});
       auto grav = [&](bool) -> cudaError_t { return mixed_gravity() ? cudaErrorUnknown : cudaSuccess; };
@@ -1010,6 +1029,7 @@ int dg_handle::mixed_autotune() {
   prof_on = prof_was;
   if (rc) return rc;
   X.tune_info = info;
+  if (stages_fixed) return DG_OK;  // a forced choice is not what the grid's tuning found
   std::lock_guard<std::mutex> lk(g_tune_mu);
   TuneVal v;
   v.hydro_kind = X.hydro_kind;
