@@ -230,9 +230,14 @@ def gravity_parts(precision, Nu, Nphi):
     g1 = 6 * Nphi * Nu * Nphi
     g1name = "phi DFT GEMM (k_gemm_split, split-BF16)"
     if Nu == 1024 and Nphi == 1024:  # fused two-stage transform: 4 rows per CTA, 2 products
-        g1 = (Nu // 4) * (6 * 128 * 128 * 32 + 6 * 128 * 64 * 64)
+        g1 = (Nu // 4) * (6 * 128 * 64 * 32 + 6 * 128 * 64 * 64)
         g1name = "fused phi transform (k_phifwd: real 32-point + complex 32-point tcgen05 stages)"
     g4 = 6 * Nu * Nphi * Nphi
+    g4name = "inverse phi DFT GEMM + potential scaling (k_gemm_split)"
+    if Nu == 1024 and Nphi == 1024:  # fused two-stage inverse: 4 rows per CTA, 2 products
+        g4 = (Nu // 4) * (6 * 128 * 64 * 64 + 6 * 128 * 32 * 64)
+        g4name = ("fused inverse phi transform (k_phiinv: complex 32-point + real-output 32-point tcgen05 "
+                  "stages, potential scaling)")
     if Nu % 1024 == 0:
         A, nm = Nu // 32, ((Nphi // 2 + 1) + 3) // 4 * 4
         u = 6 * 128 * (nm * A) * 64 + 2 * 6 * (nm * 64) * (2 * A) * (2 * A) + 6 * (nm * A) * 64 * 128
@@ -243,7 +248,7 @@ def gravity_parts(precision, Nu, Nphi):
         uname = "dense u DFT x khat (two k_gemm_split passes)"
     return [("grav_phi_fwd", g1name, "tensor", g1, "flop"),
             ("grav_u", uname, "tensor", u, "flop"),
-            ("grav_phi_inv", "inverse phi DFT GEMM + potential scaling (k_gemm_split)", "tensor", g4, "flop")]
+            ("grav_phi_inv", g4name, "tensor", g4, "flop")]
 
 
 def timed_chunks(disk, stream, flush, steps, chunk):

@@ -33,6 +33,7 @@
 #include "hydro32p.cuh"
 #include "uconv.cuh"
 #include "phifwd.cuh"
+#include "phiinv.cuh"
 
 using namespace dg;
 
@@ -87,11 +88,14 @@ struct MixedState {
   // A = 32 (Nu = 1024): the four u passes run as one fused kernel (uconv.cuh)
   bool fused_u = false;
   float *khm = nullptr;  // khat[m][p] / M, [nm][M]
-  // Nu = Nphi = 1024: the forward phi transform as one fused kernel (phifwd.cuh)
+  // Nu = Nphi = 1024: the forward and inverse phi transforms as fused kernels (phifwd.cuh,
+  // phiinv.cuh); khm then carries the inverse real DFT's weights w_m / Nphi as well
   bool fused_phi = false;
-  SplitBuf PA, PB;       // its stage-A (real 32-point) and stage-B (complex 32-point) operands
+  SplitBuf PA, PB;       // forward: stage-A (real 32-point) and stage-B (complex 32-point) operands
+  SplitBuf IA, IB;       // inverse: stage-A (complex 32-point) and stage-B (real-output 32-point) operands
+  SplitBuf Zt;           // the radial convolution's output rows, [Nu][kZtLd]
   float2 *twphi = nullptr;  // W^{m2 j1}, [32][32]
-  CUtensorMap mPA[2], mPB[2];
+  CUtensorMap mPA[2], mPB[2], mIA[2], mIB[2];
   float2 *twp = nullptr; // W_M^{p2 i1} with padded rows, [64][kUcTwLd]
   CUtensorMap mXin[2], mTb[2], mYk[2], mUb[2], mRB[2], mRA[2], mRGA[2], mRGB[2], mZmn[2];
   bool tables_ready = false;
@@ -300,12 +304,25 @@ __global__ void k_tab_phiA(SplitBuf C) {
   }
 }
 
-// KHM[m][p] = Re khat(p, m) / M for m <= Nphi/2 (padding modes: 0)
-__global__ void k_tab_khm(float *KHM, const double2 *khat, int nm, int M, int Nphi) {
+// KHM[m][p] = Re khat(p, m) / M for m <= Nphi/2 (padding modes: 0); with real_dft_weights
+// also times w_m / Nphi (w = 1 at m = 0 and Nphi/2, else 2), the inverse real DFT's weights
+__global__ void k_tab_khm(float *KHM, const double2 *khat, int nm, int M, int Nphi, bool real_dft_weights) {
   const size_t n = (size_t)nm * M;
   for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
     const int m = (int)(q / M);
-    KHM[q] = (m <= Nphi / 2) ? (float)(khat[q].x / M) : 0.f;
+    const double w = !real_dft_weights ? 1.0 : ((m == 0 || 2 * m == Nphi) ? 1.0 : 2.0) / Nphi;
+    KHM[q] = (m <= Nphi / 2) ? (float)(khat[q].x / M * w) : 0.f;
+  }
+}
+
+// stage-B operand of k_phiinv: B[j2][(m2, ri)] = cos / -sin (2 pi j2 m2 / 32), 32 x 64
+// (the real part of e^{+2 pi i j2 m2 / 32} (Y_re + i Y_im))
+__global__ void k_tab_phiIB(SplitBuf B) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 32 * 64; q += gridDim.x * blockDim.x) {
+    const int j2 = q / 64, m2 = (q % 64) >> 1, ri = q & 1;
+    double sn, cs;
+    sincospi(2.0 * (double)((j2 * m2) % 32) / 32.0, &sn, &cs);
+    put_split(B, q, ri ? -sn : cs);
   }
 }
 
@@ -630,16 +647,29 @@ int dg_handle::mixed_init() {
     k_tab_tw<<<64, 256, 0, st>>>(X.tw, A, A);
     XK(cudaGetLastError());
     X.fused_u = u_fused(Nu);
+    X.fused_phi = X.fused_u && phi_fused(Nu, Nphi);
     if (X.fused_u) {
       XK(dalloc(&X.khm, (size_t)nm * 64 * A));
       XK(dalloc(&X.twp, (size_t)64 * tc::kUcTwLd));
       k_tab_tw<<<64, 256, 0, st>>>(X.twp, A, tc::kUcTwLd);
-      k_tab_khm<<<grid_for((size_t)nm * 64 * A), 256, 0, st>>>(X.khm, Khat, nm, 64 * A, Nphi);
+      k_tab_khm<<<grid_for((size_t)nm * 64 * A), 256, 0, st>>>(X.khm, Khat, nm, 64 * A, Nphi, X.fused_phi);
       XK(cudaGetLastError());
       XK(smem_attrs((const void *)tc::k_uconv, tc::kUcSmem));
     }
-    X.fused_phi = X.fused_u && phi_fused(Nu, Nphi);
     if (X.fused_phi) {
+      static_assert(tc::kZtModes >= 1024 / 2 + 1 && tc::kZtModes % 32 == 0, "Zt row layout");
+      XK(alloc_split(X.Zt, (size_t)Nu * tc::kZtLd));
+      XK(cudaMemset(X.Zt.hi, 0, sizeof(__nv_bfloat16) * (size_t)Nu * tc::kZtLd));  // modes above Nphi/2 stay 0
+      XK(cudaMemset(X.Zt.lo, 0, sizeof(__nv_bfloat16) * (size_t)Nu * tc::kZtLd));
+      XK(alloc_split(X.IA, (size_t)64 * 64));
+      XK(alloc_split(X.IB, (size_t)32 * 64));
+      k_tab_cblock<<<32, 256, 0, st>>>(X.IA, 32, 32, 32, +1);  // W_32^{-j1 m1}
+      k_tab_phiIB<<<8, 256, 0, st>>>(X.IB);                     // Re W_32^{-j2 m2}
+      XK(cudaGetLastError());
+      bool oki = make_map(&X.mIA[0], X.IA.hi, 64, 64, tc::BN) && make_map(&X.mIA[1], X.IA.lo, 64, 64, tc::BN) &&
+                 make_map(&X.mIB[0], X.IB.hi, 32, 64, 32) && make_map(&X.mIB[1], X.IB.lo, 32, 64, 32);
+      if (!oki) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed (fused inverse phi transform)");
+      XK(smem_attrs((const void *)tc::k_phiinv, tc::kPiSmem));
       XK(alloc_split(X.PA, (size_t)64 * 64));
       XK(alloc_split(X.PB, (size_t)64 * 64));
       XK(dalloc(&X.twphi, (size_t)32 * 32));
@@ -711,7 +741,8 @@ void dg_handle::mixed_release() {
     if (X.w[b]) cudaFree(X.w[b]);
   }
   SplitBuf *bufs[] = {&X.Sx, &X.X1, &X.Wt, &X.Z, &X.Fphi, &X.Cu, &X.CuT, &X.Gphi,
-                      &X.Xin, &X.Tb, &X.Yk, &X.Ub, &X.RB, &X.RA, &X.RGA, &X.RGB, &X.PA, &X.PB};
+                      &X.Xin, &X.Tb, &X.Yk, &X.Ub, &X.RB, &X.RA, &X.RGA, &X.RGB, &X.PA, &X.PB,
+                      &X.IA, &X.IB, &X.Zt};
   for (SplitBuf *b : bufs) free_split(*b);
   void *ptrs[] = {X.KW, X.dPhi, X.rowpend, X.phiscale, X.rowbuf, X.rowbufd, X.KW2, X.tw, X.khm, X.twp, X.twphi};
   for (void *q : ptrs)
@@ -958,8 +989,10 @@ int dg_handle::mixed_autotune() {
         info += buf;
       }
     } else if (p.selfgrav) {
+      // products that run as k_gemm_split (the fused kernels have no pipeline to tune)
       const std::vector<int> slots = !X.factored ? std::vector<int>{0, 1, 2, 5}
-                                     : (X.fused_u ? std::vector<int>{0, 5} : std::vector<int>{0, 1, 2, 3, 4, 5});
+                                     : (X.fused_phi ? std::vector<int>{}
+                                        : (X.fused_u ? std::vector<int>{0, 5} : std::vector<int>{0, 1, 2, 3, 4, 5}));
       auto grav = [&](bool) -> cudaError_t { return mixed_gravity() ? cudaErrorUnknown : cudaSuccess; };
       float tbest;
       cudaError_t e = time_us(grav, &tbest);
@@ -1119,7 +1152,8 @@ int dg_handle::mixed_gravity() {
     XK(prof_begin(DG_PROF_GRAV_U));
     if (X.fused_u) {
       // F1, F2, I1, I2 in one kernel: four modes per CTA, operands kept on chip
-      tc::UconvArgs u{X.twp, X.khm, X.Z.hi, X.Z.lo, Nu, Nphi, &ctl->status};
+      tc::UconvArgs u{X.twp, X.khm, X.Z.hi, X.Z.lo, Nu, Nphi, &ctl->status,
+                      X.fused_phi ? X.Zt.hi : nullptr, X.fused_phi ? X.Zt.lo : nullptr};
       XK(launch_pdl(tc::k_uconv, dim3(nm / tc::kUcModes), dim3(tc::kUcThreads), tc::kUcSmem, st, X.mRB[0], X.mRB[1],
                     X.mXin[0], X.mXin[1], X.mRA[0], X.mRA[1], X.mRGA[0], X.mRGA[1], X.mRGB[0], X.mRGB[1], u));
     } else {
@@ -1139,17 +1173,24 @@ int dg_handle::mixed_gravity() {
       XK(gemm<tc::kEpiI2ToZ>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st, X.ns[4]));
     }
     XK(prof_end(DG_PROF_GRAV_U));
-    // G4: inverse phi DFT with Z as an MN-major operand; in a time step it arms the hydro's
-    // row-tile counters with the hydro launch's column-tile count
-    a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi; a.row_scale = X.phiscale;
-    if (X.rs_step) {
-      a.rowpend = X.rowpend;
-      a.rp_n = (Nu + kTileI - 1) / kTileI;
-      a.rp_val = X.hydro_kind == MixedState::kHydroPacked ? (Nphi + kTileJp - 1) / kTileJp : (Nphi + kTileJ - 1) / kTileJ;
-    }
+    // G4: inverse phi DFT: the fused two-stage kernel from Zt, or a product with Z as an
+    // MN-major operand; in a time step it arms the hydro's row-tile counters with the hydro
+    // launch's column-tile count
+    int *rp = X.rs_step ? X.rowpend : nullptr;
+    const int rp_n = (Nu + kTileI - 1) / kTileI;
+    const int rp_val =
+        X.hydro_kind == MixedState::kHydroPacked ? (Nphi + kTileJp - 1) / kTileJp : (Nphi + kTileJ - 1) / kTileJ;
     XK(prof_begin(DG_PROF_GRAV_PHI_INV));
-    XK((gemm<tc::kEpiRowScaleF32, true, false>(X.mZmn[0], X.mZmn[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st,
-                                               X.ns[5])));
+    if (X.fused_phi) {
+      tc::PhiInvArgs f{X.Zt.hi, X.Zt.lo, X.twphi, X.phiscale, X.dPhi, Nphi, &ctl->status, rp, rp_n, rp_val};
+      XK(launch_pdl(tc::k_phiinv, dim3(Nu / tc::kPiRows), dim3(tc::kPiThreads), tc::kPiSmem, st, X.mIA[0], X.mIA[1],
+                    X.mIB[0], X.mIB[1], f));
+    } else {
+      a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi; a.row_scale = X.phiscale;
+      a.rowpend = rp; a.rp_n = rp_n; a.rp_val = rp_val;
+      XK((gemm<tc::kEpiRowScaleF32, true, false>(X.mZmn[0], X.mZmn[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st,
+                                                 X.ns[5])));
+    }
     XK(prof_end(DG_PROF_GRAV_PHI_INV));
     return DG_OK;
   }

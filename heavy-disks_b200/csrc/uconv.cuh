@@ -37,13 +37,21 @@ constexpr int kUcTwLd = 33;          // odd row length in float2: the 64 rows fa
 constexpr uint32_t kUcTwBytes = 64 * kUcTwLd * 8;  // 16896, a multiple of 16 (one bulk copy)
 constexpr size_t kUcSmem = kUcTw + kUcTwBytes + 1024;
 constexpr uint32_t kUcTmemCols = 256;
+// Zt rows (the fused inverse phi transform's input): modes m = 0..543 as (re, im) BF16 pairs;
+// entries above Nphi / 2 = 512 stay zero
+constexpr int kZtModes = 544;
+constexpr int kZtLd = 2 * kZtModes;
 
 struct UconvArgs {
   const float2 *twiddle;  // W_M^{p2 i1}, [64][kUcTwLd] (columns 32.. unused)
   const float *khm;       // khat[m][p] / M (0 for padding modes), [nmodes][M]
-  __nv_bfloat16 *z_hi, *z_lo;  // Z[c][i], Nphi x Nu
+  __nv_bfloat16 *z_hi, *z_lo;  // Z[c][i], Nphi x Nu (dense inverse phi transform)
   int Nu, Nphi;
   int *status;
+  // when set: the output goes to Zt rows instead, [Nu][kZtLd] with mode m's (re, im) at
+  // columns 2m, 2m + 1 (the fused inverse phi transform's input, phiinv.cuh; modes above
+  // Nphi / 2 stay zero)
+  __nv_bfloat16 *zt_hi, *zt_lo;
 };
 
 // byte offset of 16-byte chunk ch of row r in a 128-byte-swizzled tile
@@ -321,8 +329,48 @@ __global__ void __launch_bounds__(kUcThreads, 1)
   ok = !abort_flag && mbar_wait(&bar_mma, 1, a.status);
   tc_fence_after();
 
-  // ---- E4: Z[c(m, ro)][i1 + 32 i2] ----
-  if (__all_sync(0xffffffffu, ok && !abort_flag)) {  // warp-uniform: tcgen05.ld is .sync.aligned
+  if (a.zt_hi) {
+    // ---- E4 (fused inverse): Zt[i][2m, 2m + 1] for the CTA's four modes.  Each (mode, row)
+    // value goes to shared memory as one word per plane, (re | im << 16), at slot
+    // mode ^ ((i >> 3) & 3) of the row's 16 bytes (the XOR keeps a warp's 32 rows on
+    // distinct banks); then one thread per row writes the row's 16 bytes per plane.  The
+    // staging area is U's (dead after S4). ----
+    uint32_t *stg = reinterpret_cast<uint32_t *>(sm + kUcU);  // [Nu][4] hi, then [Nu][4] lo
+    const int half = a.Nphi / 2;
+    if (__all_sync(0xffffffffu, ok && !abort_flag)) {
+      uint32_t v[32];
+      tmem_ld32(tl + (uint32_t)(128 + 32 * hw), v);  // columns (i2, ro), i2 = 16 hw + t / 2
+      const int m = blockIdx.x * kUcModes + q;
+      const bool live = m <= half, has_im = live && m != 0 && m != half;
+#pragma unroll
+      for (int t = 0; t < 16; ++t) {
+        const int ii = lane + 32 * (16 * hw + t);
+        uint32_t hi, lo;
+        split_pair(live ? __uint_as_float(v[2 * t]) : 0.f, has_im ? __uint_as_float(v[2 * t + 1]) : 0.f, hi, lo);
+        const int slot = q ^ ((ii >> 3) & 3);
+        stg[ii * 4 + slot] = hi;
+        stg[4 * a.Nu + ii * 4 + slot] = lo;
+      }
+    }
+    __syncthreads();
+    if (!abort_flag) {
+      const int m0 = blockIdx.x * kUcModes;
+      const int s = (threadIdx.x >> 3) & 3;  // rows threadIdx.x + 256 k share (i >> 3) & 3
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int ii = threadIdx.x + kUcThreads * k;
+#pragma unroll
+        for (int pl = 0; pl < 2; ++pl) {
+          const uint4 w = *reinterpret_cast<const uint4 *>(stg + pl * 4 * a.Nu + ii * 4);
+          auto pick = [&](int idx) { return idx == 0 ? w.x : (idx == 1 ? w.y : (idx == 2 ? w.z : w.w)); };
+          // modes m0 .. m0+3 in order
+          __nv_bfloat16 *row = (pl ? a.zt_lo : a.zt_hi) + (size_t)ii * kZtLd;
+          *reinterpret_cast<uint4 *>(row + 2 * m0) = make_uint4(pick(s), pick(1 ^ s), pick(2 ^ s), pick(3 ^ s));
+        }
+      }
+    }
+  } else if (__all_sync(0xffffffffu, ok && !abort_flag)) {  // warp-uniform: tcgen05.ld is .sync.aligned
+    // ---- E4: Z[c(m, ro)][i1 + 32 i2] ----
     uint32_t v[32];
     tmem_ld32(tl + (uint32_t)(128 + 32 * hw), v);  // columns (i2, ro), i2 = 16 hw + t / 2
     const int m = blockIdx.x * kUcModes + q, i1 = lane;
