@@ -797,7 +797,7 @@ int dg_tuning_info(const dg_handle *h, char *buf, int len) {
 int dg_kernels_per_step(const dg_handle *h) {
   if (!h) return DG_ERR_INVALID;
   const int grav = !h->p.selfgrav ? 0 : (h->p.precision == DG_PREC_MIXED ? h->mixed_gravity_kernels() : 3);
-  return grav + 1;
+  return grav + (h->p.precision == DG_PREC_MIXED ? h->mixed_hydro_kernels() : 1);
 }
 
 int dg_profile_read(dg_handle *h, double *ms, long long *count) {

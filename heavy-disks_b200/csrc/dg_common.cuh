@@ -39,7 +39,7 @@ struct Ctl {
   int ndiag;                       // per-step diagnostic rows written since the last drain
   double *diag;                    // per-step diagnostic ring (host-allocated on request), or null
   int diag_cap;                    // rows the ring holds
-  int pad2;
+  int pend_active;                 // the running hydro launch advances the state (for k_step_finalize)
   double modesum[2 * kMaxModes];   // re/im sums for the record being built
   double last_modes[2 * kMaxModes];// the most recent per-step sums (mode_every_step)
   double rec[kMaxRecords][4];      // t, |C0|, |C2|, arg C2

@@ -95,6 +95,7 @@ struct dg_handle {
   int mixed_download_state(double *Sig, double *vR, double *vp);
   int mixed_gravity();
   int mixed_gravity_kernels() const;
+  int mixed_hydro_kernels() const;
   int mixed_autotune();
   std::string mixed_tuning_info() const;
   int mixed_potential(const double *dSig, double *dOut);

@@ -29,6 +29,10 @@ struct Rows32 {
   // faces f in [0, Nu]
   const float *Af, *dRl, *dRr, *dV, *dS0;
   const float *invdR, *invdl, *invdRl, *invdRr;  // reciprocals (rows, rows, faces, faces)
+  // the packed hydro kernel's row constants, row-major [Nu + 24][20]: row r holds the
+  // constants of i = r - 3 (hydro32p.cuh), zero outside the grid, so one tile's rows are
+  // one contiguous copy
+  const float *rowtab;
   int Nu, Nphi;
   float dphi, inv2dphi, invdu, inv2du, Kpoly, gamma, gmstar;
   int gamma2;  // gamma == 2: P = K Sigma^2 exactly

@@ -45,8 +45,15 @@ constexpr int kOffSgP = 0, kOffDpP = kFieldStrideP, kOffPhP = 2 * kFieldStrideP,
               kOffW0P = 4 * kFieldStrideP;
 static_assert(kOffPhP % 32 == 0 && kOffU0P % 32 == 0 && kOffW0P % 32 == 0, "TMA destinations 128-byte aligned");
 constexpr int kOffFP = 5 * kFieldStrideP;
+// row constants: rows of the packed table Rows32::rowtab, [kRows32t][kRowTabW], one bulk copy
+constexpr int kRowTabW = 20;      // floats per table row (the tNConst constants, padded to 16 bytes)
+constexpr int kRowTabLead = 3;    // table row r holds row i = r - 3 (a tile's first staged row is i0 - 3)
+constexpr int kRowTabExtra = 24;  // table rows beyond Nu: i = -3 .. Nu + 20
+static_assert(tNConst <= kRowTabW && (kRowTabW * 4) % 16 == 0, "row table rows");
+constexpr uint32_t kRcBytesP = kRows32t * kRowTabW * 4;
 constexpr int kOffRcP = kOffFP + 4 * kFaceArr32t;
-constexpr size_t kSmem32p = (size_t)(kOffRcP + tNConst * kRows32t) * sizeof(float) + 128;  // + alignment slack
+static_assert(kOffRcP % 4 == 0, "bulk-copy destination 16-byte aligned");
+constexpr size_t kSmem32p = (size_t)(kOffRcP + kRows32t * kRowTabW) * sizeof(float) + 128;  // + alignment slack
 constexpr uint32_t kFieldBytesP = kFieldP * 4;
 
 namespace p2 {
@@ -78,7 +85,7 @@ __device__ __forceinline__ void hydro32p_tile(
     const float *__restrict__ Phi, const double *__restrict__ gRin, const double *__restrict__ gpin,
     float *__restrict__ so, float *__restrict__ uo, float *__restrict__ wo, const SplitBf16 &Sx, Ctl *ctl,
     const Rows32 &g, float *sm32t, double *red, double *bsum, double *zsum, const CUtensorMap *tmS,
-    const CUtensorMap *tmU, const CUtensorMap *tmW, const CUtensorMap *tmP, uint64_t *bar_ld) {
+    const CUtensorMap *tmU, const CUtensorMap *tmW, const CUtensorMap *tmP, uint64_t *bar_ld, uint64_t *bar_rc) {
   using namespace p2;
   float *rc = sm32t + kOffRcP;
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
@@ -106,39 +113,14 @@ __device__ __forceinline__ void hydro32p_tile(
   // output columns c in [3, 61) with J = xs0 + c <= Nphi: .x on lanes 2..30, .y on lanes 1..29
   const bool outx = lane >= 2 && lane <= 30 && xs0 + 2 * lane <= Nphi;
   const bool outy = lane >= 1 && lane <= 29 && xs0 + 2 * lane + 1 <= Nphi;
-#define RC(k, i) rc[(k) * kRows32t + (i) - ib]
+#define RC(k, i) rc[((i) - ib) * kRowTabW + (k)]
   auto row_ok = [&](int i) { return IN || (i >= 0 && i < Nu); };
   auto first_row = [&](int i) { return !IN && i == 0; };
   auto last_row = [&](int i) { return !IN && i == Nu - 1; };
 
-  for (int t = tid; t < tNConst * kRows32t; t += kThreads32t) {
-    const int k = t / kRows32t, r = t - k * kRows32t, i = ib + r;
-    float v = 0.f;
-    if (i >= 0 && i <= Nu) {
-      const bool row = i < Nu;
-      switch (k) {
-        case tS0: v = row ? g.S0[i] : 0.f; break;
-        case tInvS0: v = row ? g.invS0[i] : 0.f; break;
-        case tV0: v = row ? g.V0[i] : 0.f; break;
-        case tA0: v = row ? g.a0[i] : 0.f; break;
-        case tDP0: v = row ? g.dP0dR[i] : 0.f; break;
-        case tInvdRc: v = row ? g.invdRc[i] : 0.f; break;
-        case tInvR: v = row ? g.invR[i] : 0.f; break;
-        case tR: v = row ? g.R[i] : 0.f; break;
-        case tInvVol: v = row ? g.invVol[i] : 0.f; break;
-        case tInvdl: v = row ? g.invdl[i] : 0.f; break;
-        case tAphi: v = row ? g.Aphi[i] : 0.f; break;
-        case tR32: v = row ? g.R32[i] : 0.f; break;
-        case tInvdR: v = row ? g.invdR[i] : 0.f; break;
-        case tP0: v = row ? g.P0[i] : 0.f; break;
-        case tDS0: v = g.dS0[i]; break;
-        case tDV: v = g.dV[i]; break;
-        case tAf: v = g.Af[i]; break;
-        case tInvdRl: v = g.invdRl[i]; break;
-        case tInvdRr: v = g.invdRr[i]; break;
-      }
-    }
-    rc[t] = v;
+  if (tid == 0) {  // the tile's row constants: constant tables, independent of the previous kernel
+    tc::mbar_arrive_expect_tx(bar_rc, kRcBytesP);
+    tc::bulk_load(rc, g.rowtab + (size_t)(ib + kRowTabLead) * kRowTabW, kRcBytesP, bar_rc);
   }
   if (tid < 2 * kMaxModes) {
     bsum[tid] = 0.0;
@@ -156,32 +138,10 @@ __device__ __forceinline__ void hydro32p_tile(
     tc::tma_load_2d(sm32t + kOffW0P, tmW, bar_ld, xa, ib);
     if (FM == kForcePhi) tc::tma_load_2d(sm32t + kOffPhP, tmP, bar_ld, xa, ib);
   }
-  const StepInfo si = read_step_info(ctl, true);
-  const float dt = (float)si.dt;
+  // the step's control fields: loaded now, used once the tile has landed
+  const StepRaw sraw = load_step_raw(ctl);
   float lmaxf = 0.f;
   bool bad = false;
-
-  if (!si.active) {
-    if (use_tma && tid == 0) tc::mbar_wait(bar_ld, 0, &ctl->status);  // no copy in flight at exit
-    // pass-through: copy the tile and report the CFL rate of the unchanged state
-#pragma unroll
-    for (int k = 0; k < kItOutP; ++k) {
-      const int i = i0 + wp + kWarps32p * k;
-      if (i < Nu) {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          if (e == 0 ? outx : outy) {
-            const size_t q = (size_t)i * Nphi + jc + e;
-            so[q] = sig[q]; uo[q] = uu[q]; wo[q] = ww[q];
-            lmaxf = fmaxf(lmaxf, cfl_rate32(g, i, sig[q], uu[q], ww[q]));
-          }
-        }
-      }
-    }
-    __syncthreads();
-    finish_launch<kThreads32t>(ctl, si, (double)lmaxf, tid == 0 ? bsum : zsum, red);
-    return;
-  }
 
   // ---- S0 (edge tiles, caller forces): the same rows by thread loads ----
   if (!use_tma) {
@@ -209,12 +169,42 @@ __device__ __forceinline__ void hydro32p_tile(
       }
     }
   }
-  __syncthreads();  // row constants (and thread-loaded fields) staged
-  if (use_tma && !tc::mbar_wait(bar_ld, 0, &ctl->status)) {
-    // the copies did not land in time: the step is void (status raised); wait once more
-    // (bounded) so that no copy is in flight when the CTA exits, then go on with the rest
-    if (tid == 0) tc::mbar_wait(bar_ld, 0, &ctl->status);
+  __syncthreads();  // thread-loaded fields staged
+  {
+    bool landed = tc::mbar_wait(bar_rc, 0, &ctl->status);
+    if (use_tma) landed = tc::mbar_wait(bar_ld, 0, &ctl->status) && landed;
+    if (!landed && tid == 0) {
+      // the copies did not land in time: the step is void (status raised); wait once more
+      // (bounded) so that no copy is in flight when the CTA exits, then go on with the rest
+      tc::mbar_wait(bar_rc, 0, &ctl->status);
+      if (use_tma) tc::mbar_wait(bar_ld, 0, &ctl->status);
+    }
   }
+  const StepInfo si = step_info_from(sraw, true);
+  const float dt = (float)si.dt;
+
+  if (!si.active) {
+    // pass-through: copy the tile and report the CFL rate of the unchanged state
+#pragma unroll
+    for (int k = 0; k < kItOutP; ++k) {
+      const int i = i0 + wp + kWarps32p * k;
+      if (i < Nu) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          if (e == 0 ? outx : outy) {
+            const size_t q = (size_t)i * Nphi + jc + e;
+            so[q] = sig[q]; uo[q] = uu[q]; wo[q] = ww[q];
+            lmaxf = fmaxf(lmaxf, cfl_rate32(g, i, sig[q], uu[q], ww[q]));
+          }
+        }
+      }
+    }
+    __syncthreads();
+    finish_launch_deferred<kThreads32t>(ctl, si, (double)lmaxf, tid == 0 ? bsum : zsum, red);
+    return;
+  }
+
+  // ---- S1: pressure perturbation dP of the staged rows ----
 #pragma unroll
   for (int k = 0; k < kItLoadP; ++k) {
     const int r = wp + kWarps32p * k, i = ib + r;
@@ -497,7 +487,7 @@ __device__ __forceinline__ void hydro32p_tile(
   __syncthreads();
   double lmax = (double)lmaxf;
   if (bad) lmax = __longlong_as_double(0x7ff8000000000000ll);
-  finish_launch<kThreads32t>(ctl, si, lmax, tid == 0 ? bsum : zsum, red);
+  finish_launch_deferred<kThreads32t>(ctl, si, lmax, tid == 0 ? bsum : zsum, red);
 #undef RC
 }
 
@@ -514,19 +504,20 @@ __global__ void __launch_bounds__(kThreads32t, 4) k_hydro32p(
   float *sm32t = reinterpret_cast<float *>(((uintptr_t)sm32p_raw + 127) & ~(uintptr_t)127);
   __shared__ double red[kThreads32t / 32];
   __shared__ double bsum[2 * kMaxModes], zsum[2 * kMaxModes];
-  __shared__ __align__(8) uint64_t bar_ld;
+  __shared__ __align__(8) uint64_t bar_ld, bar_rc;
   if (threadIdx.x == 0) {
     tc::mbar_init(&bar_ld, 1);
+    tc::mbar_init(&bar_rc, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   // (the first CTA barrier inside the tile function orders the set-up before any wait)
   const int i0 = blockIdx.y * kTileI;
   if (i0 >= 3 && i0 + kTileI + 3 <= g.Nu)
     hydro32p_tile<G2, FM, true>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum, &tmS,
-                                &tmU, &tmW, &tmP, &bar_ld);
+                                &tmU, &tmW, &tmP, &bar_ld, &bar_rc);
   else
     hydro32p_tile<G2, FM, false>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum, &tmS,
-                                 &tmU, &tmW, &tmP, &bar_ld);
+                                 &tmU, &tmW, &tmP, &bar_ld, &bar_rc);
   if (rowpend) rowtile_done(rowpend + blockIdx.y);  // this tile's outputs are written
 }
 

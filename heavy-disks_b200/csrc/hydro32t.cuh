@@ -139,7 +139,7 @@ __device__ __forceinline__ void hydro32t_tile(
       }
     }
     __syncthreads();
-    finish_launch<kThreads32t>(ctl, si, (double)lmaxf, tid == 0 ? bsum : zsum, red);
+    finish_launch_deferred<kThreads32t>(ctl, si, (double)lmaxf, tid == 0 ? bsum : zsum, red);
     return;
   }
 
@@ -379,7 +379,7 @@ __device__ __forceinline__ void hydro32t_tile(
   __syncthreads();
   double lmax = (double)lmaxf;
   if (bad) lmax = __longlong_as_double(0x7ff8000000000000ll);
-  finish_launch<kThreads32t>(ctl, si, lmax, tid == 0 ? bsum : zsum, red);
+  finish_launch_deferred<kThreads32t>(ctl, si, lmax, tid == 0 ? bsum : zsum, red);
 #undef RC
 }
 

@@ -49,6 +49,7 @@ struct MixedState {
   int Nu = 0, Nphi = 0;
   // per-row / per-face tables
   float *rowbuf = nullptr;    // packed FP32 row and face arrays
+  float *rowtab = nullptr;    // the same constants row-major for k_hydro32p (Rows32::rowtab)
   double *rowbufd = nullptr;  // packed FP64 row arrays
   Rows32 rows{};
   std::vector<double> S0, V0, g0;  // FP64 basic state (host)
@@ -600,6 +601,7 @@ int dg_handle::mixed_init() {
   XK(cudaMemsetAsync(X.rowpend, 0, (size_t)(Nu + kTileI - 1) / kTileI * sizeof(int), st));
   XK(dalloc(&X.phiscale, Nu));
   XK(dalloc(&X.rowbuf, (size_t)24 * (Nu + 1)));
+  XK(dalloc(&X.rowtab, (size_t)(Nu + kRowTabExtra) * kRowTabW));
   XK(dalloc(&X.rowbufd, (size_t)4 * Nu));
   // DFT tables
   k_tab_phi<<<grid_for((size_t)Nphi * Nphi), 256, 0, st>>>(X.Fphi, X.Gphi, Nphi);
@@ -744,7 +746,7 @@ void dg_handle::mixed_release() {
                       &X.Xin, &X.Tb, &X.Yk, &X.Ub, &X.RB, &X.RA, &X.RGA, &X.RGB, &X.PA, &X.PB,
                       &X.IA, &X.IB, &X.Zt};
   for (SplitBuf *b : bufs) free_split(*b);
-  void *ptrs[] = {X.KW, X.dPhi, X.rowpend, X.phiscale, X.rowbuf, X.rowbufd, X.KW2, X.tw, X.khm, X.twp, X.twphi};
+  void *ptrs[] = {X.KW, X.dPhi, X.rowpend, X.phiscale, X.rowbuf, X.rowtab, X.rowbufd, X.KW2, X.tw, X.khm, X.twp, X.twphi};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   delete mx;
@@ -841,7 +843,19 @@ static int build_basic(dg_handle *h, const double *Sig, const double *vp) {
     rd[2 * Nu + i] = R[i];
     rd[3 * Nu + i] = R[i] * (Rf[i + 1] - Rf[i]) * h->dphi;
   }
+  // row-major copy for k_hydro32p: row r = i + kRowTabLead, the tile kernels' row constants
+  // (zero outside the grid; face arrays are defined up to i = Nu)
+  static const int rt_col[tNConst] = {4, 5, 6, 7, 3, 2, 1, 0, 11, 20, 10, 12, 19, 13, 18, 17, 14, 21, 22};
+  std::vector<float> rt((size_t)(Nu + kRowTabExtra) * kRowTabW, 0.f);
+  for (int r = 0; r < Nu + kRowTabExtra; ++r) {
+    const int i = r - kRowTabLead;
+    for (int k = 0; k < tNConst; ++k) {
+      const bool face = k >= tDS0;
+      if (i >= 0 && (face ? i <= Nu : i < Nu)) rt[(size_t)r * kRowTabW + k] = col(rt_col[k])[i];
+    }
+  }
   if (cudaMemcpyAsync(X.rowbuf, rb.data(), rb.size() * sizeof(float), cudaMemcpyHostToDevice, h->st) != cudaSuccess ||
+      cudaMemcpyAsync(X.rowtab, rt.data(), rt.size() * sizeof(float), cudaMemcpyHostToDevice, h->st) != cudaSuccess ||
       cudaMemcpyAsync(X.rowbufd, rd.data(), rd.size() * sizeof(double), cudaMemcpyHostToDevice, h->st) != cudaSuccess)
     return h->fail(DG_ERR_CUDA, "basic state", "row tables");
   Rows32 &g = X.rows;
@@ -851,6 +865,7 @@ static int build_basic(dg_handle *h, const double *Sig, const double *vp) {
   g.a0 = dc(7); g.dR = dc(8); g.dl = dc(9); g.Aphi = dc(10); g.invVol = dc(11); g.R32 = dc(12); g.P0 = dc(13);
   g.Af = dc(14); g.dRl = dc(15); g.dRr = dc(16); g.dV = dc(17); g.dS0 = dc(18);
   g.invdR = dc(19); g.invdl = dc(20); g.invdRl = dc(21); g.invdRr = dc(22);
+  g.rowtab = X.rowtab;
   g.S0d = X.rowbufd; g.V0d = X.rowbufd + Nu; g.Rd = X.rowbufd + 2 * Nu; g.dAd = X.rowbufd + 3 * Nu;
   g.Nu = Nu; g.Nphi = Nphi;
   g.dphi = (float)h->dphi; g.inv2dphi = (float)(1.0 / (2.0 * h->dphi));
@@ -1086,6 +1101,14 @@ int dg_handle::mixed_download_state(double *Sig, double *vRh, double *vph) {
   return DG_OK;
 }
 
+// End of a tile hydro launch: t, dt, records and diagnostics from the sums its CTAs folded
+// into the control block (step_ctl.cuh finish_launch_deferred).
+__global__ void k_step_finalize(Ctl *ctl) {
+  pdl_trigger();  // the next kernel's prologue may start; it waits for this one's completion
+  pdl_wait();     // every CTA of the hydro launch has folded its sums
+  if (threadIdx.x == 0) finalize_launch(ctl, read_step_info(ctl, true, ctl->pend_active));
+}
+
 static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *u, const float *w, const float *Phi,
                                   const double *gR, const double *gp, int fm, float *so, float *uo, float *wo, Ctl *ctl,
                                   cudaStream_t st, int *rowpend) {
@@ -1102,6 +1125,7 @@ static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *
     if (fm == kForcePhi) g2 ? go(k_hydro32p<true, kForcePhi>) : go(k_hydro32p<false, kForcePhi>);
     else if (fm == kForceArrays) g2 ? go(k_hydro32p<true, kForceArrays>) : go(k_hydro32p<false, kForceArrays>);
     else g2 ? go(k_hydro32p<true, kForceNone>) : go(k_hydro32p<false, kForceNone>);
+    if (e == cudaSuccess) e = launch_pdl(k_step_finalize, dim3(1), dim3(32), 0, st, ctl);
     return e;
   }
   if (X.hydro_kind == MixedState::kHydroTile) {
@@ -1116,6 +1140,7 @@ static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *
     if (fm == kForcePhi) g2 ? go(k_hydro32t<true, kForcePhi>) : go(k_hydro32t<false, kForcePhi>);
     else if (fm == kForceArrays) g2 ? go(k_hydro32t<true, kForceArrays>) : go(k_hydro32t<false, kForceArrays>);
     else g2 ? go(k_hydro32t<true, kForceNone>) : go(k_hydro32t<false, kForceNone>);
+    if (e == cudaSuccess) e = launch_pdl(k_step_finalize, dim3(1), dim3(32), 0, st, ctl);
     return e;
   }
   if (rowpend) return cudaErrorInvalidValue;  // the warp form has no row-tile hand-over
@@ -1213,6 +1238,11 @@ int dg_handle::mixed_gravity() {
   XK(gemm<tc::kEpiRowScaleF32>(X.mZ[0], X.mZ[1], X.mGphi[0], X.mGphi[1], Nu, Nphi, Nphi, a, st, X.ns[5]));
   XK(prof_end(DG_PROF_GRAV_PHI_INV));
   return DG_OK;
+}
+
+// the tile forms end with k_step_finalize
+int dg_handle::mixed_hydro_kernels() const {
+  return (mx && mx->hydro_kind != MixedState::kHydroWarp) ? 2 : 1;
 }
 
 int dg_handle::mixed_gravity_kernels() const {

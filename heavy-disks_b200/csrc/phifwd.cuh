@@ -191,6 +191,9 @@ __global__ void __launch_bounds__(kPfThreads, 2)
     }
   }
   if (threadIdx.x == 0 && !in_seen) mbar_wait(&bar_in, 0, a.status);  // copies in flight land first
+  // with the row-tile hand-over this kernel never waited for its predecessor (the step's
+  // finalisation); waiting now makes this kernel's completion imply that one's
+  if (a.rowpend) pdl_wait();
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, kPfTmemCols);

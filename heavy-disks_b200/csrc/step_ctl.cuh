@@ -19,28 +19,55 @@ struct StepInfo {
   int nmodes;      // number of m accumulated (0 = none)
 };
 
-__device__ __forceinline__ StepInfo read_step_info(const Ctl *ctl, bool advance_t) {
+// The control-block fields a launch decides on, loaded in one go (a kernel can issue these
+// loads early and derive its StepInfo after other waits).
+struct StepRaw {
+  double t, dt, tlim, tnext;
+  int status, fixed_dt, mode_every_step, mmax;
+};
+__device__ __forceinline__ StepRaw load_step_raw(const Ctl *ctl) {
+  StepRaw r;
+  r.t = ctl->t;
+  r.dt = ctl->dt;
+  r.tlim = ctl->tlim;
+  r.tnext = ctl->tnext;
+  r.status = ctl->status;
+  r.fixed_dt = ctl->fixed_dt;
+  r.mode_every_step = ctl->mode_every_step;
+  r.mmax = ctl->mmax;
+  return r;
+}
+
+// force_active >= 0 replaces the status / tlim test (k_step_finalize: the decision the hydro
+// launch took at its start, before its own CTAs could raise status bits)
+__device__ __forceinline__ StepInfo step_info_from(const StepRaw &r, bool advance_t, int force_active = -1) {
   StepInfo s;
-  s.t = ctl->t;
-  s.dt = ctl->dt;
-  s.tlim = ctl->tlim;
+  s.t = r.t;
+  s.dt = r.dt;
+  s.tlim = r.tlim;
   s.advance_t = advance_t;
-  s.active = (ctl->status == 0) && (ctl->fixed_dt || s.t < s.tlim);
+  s.active = force_active >= 0 ? force_active != 0 : (r.status == 0) && (r.fixed_dt || s.t < s.tlim);
   s.record = false;
   s.nmodes = 0;
-  if (advance_t && s.active && !ctl->fixed_dt) {
+  if (advance_t && s.active && !r.fixed_dt) {
     double tn = s.t + s.dt;
-    s.record = (tn < s.tlim) && (tn >= ctl->tnext - 1e-12);
+    s.record = (tn < s.tlim) && (tn >= r.tnext - 1e-12);
   }
   if (s.record) s.nmodes = 3;  // C0, C1, C2
-  if (ctl->mode_every_step && s.active) s.nmodes = ctl->mmax + 1 > s.nmodes ? ctl->mmax + 1 : s.nmodes;
+  if (r.mode_every_step && s.active) s.nmodes = r.mmax + 1 > s.nmodes ? r.mmax + 1 : s.nmodes;
   if (s.nmodes > kMaxModes) s.nmodes = kMaxModes;
   return s;
 }
 
+__device__ __forceinline__ StepInfo read_step_info(const Ctl *ctl, bool advance_t, int force_active = -1) {
+  return step_info_from(load_step_raw(ctl), advance_t, force_active);
+}
+
+// A CTA's share of the launch: its CFL max and mode sums, folded into the control block
+// with fire-and-forget atomics (the result of thread 0's block reduction).
 template <int NT>
-__device__ __forceinline__ void finish_launch(Ctl *ctl, const StepInfo &si, double local_max, const double *msum, double *red) {
-  __shared__ bool am_last;
+__device__ __forceinline__ double fold_launch_sums(Ctl *ctl, const StepInfo &si, double local_max, const double *msum,
+                                                   double *red) {
   double bmax = block_max_nan<NT>(local_max, red);
   // mode sums: block reduce each component
   for (int q = 0; q < 2 * si.nmodes; ++q) {
@@ -54,8 +81,19 @@ __device__ __forceinline__ void finish_launch(Ctl *ctl, const StepInfo &si, doub
     }
     __syncthreads();
   }
+  if (threadIdx.x == 0) atomic_max_pos(&ctl->dtinv_bits, bmax);
+  return bmax;
+}
+
+// The end of a launch: t, dt, records and diagnostics from the folded sums (thread 0 of
+// the last CTA, or k_step_finalize after the whole launch).
+__device__ __forceinline__ void finalize_launch(Ctl *ctl, const StepInfo &si);
+
+template <int NT>
+__device__ __forceinline__ void finish_launch(Ctl *ctl, const StepInfo &si, double local_max, const double *msum, double *red) {
+  __shared__ bool am_last;
+  fold_launch_sums<NT>(ctl, si, local_max, msum, red);
   if (threadIdx.x == 0) {
-    atomic_max_pos(&ctl->dtinv_bits, bmax);
     __threadfence();
     unsigned prev = atomicAdd(&ctl->done_ctas, 1u);
     am_last = (prev == gridDim.x * gridDim.y - 1);
@@ -63,6 +101,20 @@ __device__ __forceinline__ void finish_launch(Ctl *ctl, const StepInfo &si, doub
   __syncthreads();
   if (!am_last || threadIdx.x != 0) return;
   __threadfence();
+  finalize_launch(ctl, si);
+}
+
+// Deferred end of launch (the mixed tile hydro kernels): the CTAs only fold their sums;
+// k_step_finalize, launched right after with programmatic dependence, waits for the whole
+// launch and finalises, so no CTA waits on a control-block round trip before it exits.
+template <int NT>
+__device__ __forceinline__ void finish_launch_deferred(Ctl *ctl, const StepInfo &si, double local_max,
+                                                       const double *msum, double *red) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0) ctl->pend_active = si.active ? 1 : 0;
+  fold_launch_sums<NT>(ctl, si, local_max, msum, red);
+}
+
+__device__ __forceinline__ void finalize_launch(Ctl *ctl, const StepInfo &si) {
   double dtinv = __longlong_as_double((long long)atomicAdd(&ctl->dtinv_bits, 0ull));
   dtinv = (dtinv < 1e-30) ? 1e-30 : dtinv;  // reduction starts at 1e-30 (hydro.hpp:49)
   double t = si.t;

@@ -72,13 +72,6 @@ __device__ __forceinline__ void split_pair(float re, float im, uint32_t &hi, uin
   lo = pack_bf16(rl, il);
 }
 
-// one contiguous global -> shared copy completing on an mbarrier (16-byte aligned, size % 16 == 0)
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"((uint64_t)src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
 
 __device__ __forceinline__ void mma3(uint32_t d, uint64_t ah, uint64_t al, uint64_t bh, uint64_t bl, uint32_t idesc,
                                      bool first) {

@@ -232,8 +232,9 @@ int dg_step_host(dg_handle *h, double cfl, double *Sig, double *vR, double *vp, 
 int dg_profile_enable(dg_handle *h, int on);
 /* Accumulated milliseconds and launch counts per phase since the last read (resets). */
 int dg_profile_read(dg_handle *h, double *ms, long long *count);
-/* Number of this library's kernels one time step of the handle launches (gravity passes
- * plus the fused hydro kernel); depends on precision, grid and self-gravity. */
+/* Number of this library's kernels one time step of the handle launches (gravity passes,
+ * the fused hydro kernel and, after the mixed path's tile hydro forms, the one-warp step
+ * finalisation); depends on precision, grid, hydro form and self-gravity. */
 int dg_kernels_per_step(const dg_handle *h);
 /* What the autotuner chose for this handle, as one line of text (NUL-terminated, cut to
  * len bytes): the hydro kernel form and the pipeline depth of each gravity product, with
