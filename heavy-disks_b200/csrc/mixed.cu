@@ -707,9 +707,9 @@ int dg_handle::mixed_init() {
   XK(cudaStreamSynchronize(st));
   {
     const char *hk = getenv("DISKGPU_HYDRO32");
-    X.hydro_kind = MixedState::kHydroTile;
+    X.hydro_kind = MixedState::kHydroPacked;
     if (hk && strcmp(hk, "warp") == 0) X.hydro_kind = MixedState::kHydroWarp;
-    if (hk && strcmp(hk, "packed") == 0) X.hydro_kind = MixedState::kHydroPacked;
+    if (hk && strcmp(hk, "tile") == 0) X.hydro_kind = MixedState::kHydroTile;
     if (Nphi < kLd32t || Nphi % 2) X.hydro_kind = MixedState::kHydroWarp;
     if (X.hydro_kind != MixedState::kHydroWarp) {
       XK(hydro32t_prepare());
@@ -914,7 +914,7 @@ int dg_handle::mixed_upload_state(const double *Sig, const double *vRh, const do
 //     buffers and a scratch control block, so the handle's dt, time and records are untouched.
 // A variant must beat the current choice by 2 % to replace it.  Choices are cached per
 // process by (Nu, Nphi, Gamma = 2, self-gravity), so the disks of a batch that share a grid
-// are tuned once.  DISKGPU_TUNE=0 keeps the defaults (tiled hydro, stages by K);
+// are tuned once.  DISKGPU_TUNE=0 keeps the defaults (packed hydro, stages by K);
 // DISKGPU_HYDRO32 fixes the hydro form.
 namespace {
 struct TuneKey {
@@ -1049,9 +1049,12 @@ int dg_handle::mixed_autotune() {
         return launch_hydro32(X, X.sig[c], X.u[c], X.w[c], X.dPhi, nullptr, nullptr, fm, X.sig[o], X.u[o], X.w[o],
                               sctl, st);
       };
-      const int kinds[3] = {MixedState::kHydroTile, MixedState::kHydroPacked, MixedState::kHydroWarp};
+      // the packed form first: it is timed alone here, but inside a step its TMA-staged tile,
+      // bulk-copied row constants and early control loads overlap the kernels around it, so
+      // another form must beat it by the margin alone
+      const int kinds[3] = {MixedState::kHydroPacked, MixedState::kHydroTile, MixedState::kHydroWarp};
       float tk[3] = {0.f, 0.f, 0.f};
-      int best = MixedState::kHydroTile;
+      int best = MixedState::kHydroPacked;
       float tb = 1e30f;
       cudaError_t e = cudaSuccess;
       for (int q = 0; q < 3 && e == cudaSuccess; ++q) {
@@ -1064,7 +1067,7 @@ int dg_handle::mixed_autotune() {
       }
       X.hydro_kind = best;
       if (e != cudaSuccess) { rc = fail(DG_ERR_CUDA, "autotune", cudaGetErrorString(e)); break; }
-      snprintf(buf, sizeof buf, "%shydro %s (tile %.1f us, packed %.1f us, warp %.1f us)", info.empty() ? "" : "; ",
+      snprintf(buf, sizeof buf, "%shydro %s (packed %.1f us, tile %.1f us, warp %.1f us)", info.empty() ? "" : "; ",
                kHydroNames[best], tk[0], tk[1], tk[2]);
       info += buf;
     } else {
