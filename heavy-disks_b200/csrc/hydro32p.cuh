@@ -409,23 +409,24 @@ __device__ __forceinline__ void hydro32p_tile(
         const size_t q = (size_t)i * Nphi + jc;
         const float R32 = RC(tR32, i);
         const F2 xr = mul(S(R32), s3);
-        const __nv_bfloat16 hx = __float2bfloat16_rn(xr.x), hy = __float2bfloat16_rn(xr.y);
-        const __nv_bfloat16 lx = __float2bfloat16_rn(xr.x - __bfloat162float(hx));
-        const __nv_bfloat16 ly = __float2bfloat16_rn(xr.y - __bfloat162float(hy));
+        // split-BF16 operand: one packed conversion per plane, the roundings of split_bf16
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(xr.x, xr.y);
+        const float2 hf = __bfloat1622float2(h2);
+        const __nv_bfloat162 l2 = __floats2bfloat162_rn(xr.x - hf.x, xr.y - hf.y);
         if (outx && outy) {
           *reinterpret_cast<F2 *>(so + q) = s3;
           *reinterpret_cast<F2 *>(uo + q) = u3;
           *reinterpret_cast<F2 *>(wo + q) = w3;
-          *reinterpret_cast<__nv_bfloat162 *>(Sx.hi + q) = __halves2bfloat162(hx, hy);
-          *reinterpret_cast<__nv_bfloat162 *>(Sx.lo + q) = __halves2bfloat162(lx, ly);
+          *reinterpret_cast<__nv_bfloat162 *>(Sx.hi + q) = h2;
+          *reinterpret_cast<__nv_bfloat162 *>(Sx.lo + q) = l2;
         } else if (outx) {  // one half of the pair is output (tile edges)
           so[q] = s3.x; uo[q] = u3.x; wo[q] = w3.x;
-          Sx.hi[q] = hx;
-          Sx.lo[q] = lx;
+          Sx.hi[q] = h2.x;
+          Sx.lo[q] = l2.x;
         } else {
           so[q + 1] = s3.y; uo[q + 1] = u3.y; wo[q + 1] = w3.y;
-          Sx.hi[q + 1] = hy;
-          Sx.lo[q + 1] = ly;
+          Sx.hi[q + 1] = h2.y;
+          Sx.lo[q + 1] = l2.y;
         }
         // CFL rate of the new state (hydro.hpp:54-57)
         const F2 scl = make_float2(flx ? 1e-10f : sn3.x, fly ? 1e-10f : sn3.y);

@@ -178,14 +178,13 @@ __global__ void __launch_bounds__(kPfThreads, 2)
       const int m = m2 + 32 * (16 * hw + t);
       if (m <= half) {
         const size_t col = (size_t)m * 32 + i1;
-        __nv_bfloat16 h, l;
-        split_bf16(__uint_as_float(v[2 * t]), h, l);
-        a.xin_hi[rre + col] = h;
-        a.xin_lo[rre + col] = l;
+        uint32_t h, l;  // (re | im << 16) per plane
+        split_pair(__uint_as_float(v[2 * t]), __uint_as_float(v[2 * t + 1]), h, l);
+        reinterpret_cast<uint16_t *>(a.xin_hi)[rre + col] = (uint16_t)h;
+        reinterpret_cast<uint16_t *>(a.xin_lo)[rre + col] = (uint16_t)l;
         if (m != 0 && m != half) {  // self-conjugate modes have no imaginary part
-          split_bf16(__uint_as_float(v[2 * t + 1]), h, l);
-          a.xin_hi[rim + col] = h;
-          a.xin_lo[rim + col] = l;
+          reinterpret_cast<uint16_t *>(a.xin_hi)[rim + col] = (uint16_t)(h >> 16);
+          reinterpret_cast<uint16_t *>(a.xin_lo)[rim + col] = (uint16_t)(l >> 16);
         }
       }
     }

@@ -64,12 +64,13 @@ __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) 
 }
 
 // split a complex value into its hi and lo (re, im) BF16 words
+// (one packed two-value conversion per plane; the same roundings as split_bf16 on each)
 __device__ __forceinline__ void split_pair(float re, float im, uint32_t &hi, uint32_t &lo) {
-  __nv_bfloat16 rh, rl, ih, il;
-  split_bf16(re, rh, rl);
-  split_bf16(im, ih, il);
-  hi = pack_bf16(rh, ih);
-  lo = pack_bf16(rl, il);
+  const __nv_bfloat162 h = __floats2bfloat162_rn(re, im);  // .x (low half) = re
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(re - hf.x, im - hf.y);
+  hi = *reinterpret_cast<const uint32_t *>(&h);
+  lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
 
