@@ -85,7 +85,8 @@ __device__ __forceinline__ void hydro32p_tile(
     const float *__restrict__ Phi, const double *__restrict__ gRin, const double *__restrict__ gpin,
     float *__restrict__ so, float *__restrict__ uo, float *__restrict__ wo, const SplitBf16 &Sx, Ctl *ctl,
     const Rows32 &g, float *sm32t, double *red, double *bsum, double *zsum, const CUtensorMap *tmS,
-    const CUtensorMap *tmU, const CUtensorMap *tmW, const CUtensorMap *tmP, uint64_t *bar_ld, uint64_t *bar_rc) {
+    const CUtensorMap *tmU, const CUtensorMap *tmW, const CUtensorMap *tmP, uint64_t *bar_ld, uint64_t *bar_rc,
+    bool early_state) {
   using namespace p2;
   float *rc = sm32t + kOffRcP;
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
@@ -126,16 +127,26 @@ __device__ __forceinline__ void hydro32p_tile(
     bsum[tid] = 0.0;
     zsum[tid] = 0.0;
   }
-  pdl_wait();  // dt, the state and dPhi come from earlier kernels on the stream
-  pdl_trigger();
   // ---- S0 (interior column tiles): sigma, u, w, dPhi of rows i0-3 .. i0+kTileI+2 by TMA,
-  // issued before the step info is read so that the two latencies overlap ----
-  if (use_tma && tid == 0) {
-    const int xa = xs0 - 2 * po;  // a multiple of 4 columns (16 bytes)
+  // issued before the step info is read so that the two latencies overlap.  With
+  // early_state (a time step whose previous kernel only wrote dPhi, so the state's writer
+  // completed before it started) the state's boxes go out before the dependence wait. ----
+  const int xa = xs0 - 2 * po;  // a multiple of 4 columns (16 bytes)
+  if (use_tma && tid == 0 && early_state) {
     tc::mbar_arrive_expect_tx(bar_ld, (FM == kForcePhi ? 4u : 3u) * kFieldBytesP);
     tc::tma_load_2d(sm32t + kOffSgP, tmS, bar_ld, xa, ib);
     tc::tma_load_2d(sm32t + kOffU0P, tmU, bar_ld, xa, ib);
     tc::tma_load_2d(sm32t + kOffW0P, tmW, bar_ld, xa, ib);
+  }
+  pdl_wait();  // dt, the state and dPhi come from earlier kernels on the stream
+  pdl_trigger();
+  if (use_tma && tid == 0) {
+    if (!early_state) {
+      tc::mbar_arrive_expect_tx(bar_ld, (FM == kForcePhi ? 4u : 3u) * kFieldBytesP);
+      tc::tma_load_2d(sm32t + kOffSgP, tmS, bar_ld, xa, ib);
+      tc::tma_load_2d(sm32t + kOffU0P, tmU, bar_ld, xa, ib);
+      tc::tma_load_2d(sm32t + kOffW0P, tmW, bar_ld, xa, ib);
+    }
     if (FM == kForcePhi) tc::tma_load_2d(sm32t + kOffPhP, tmP, bar_ld, xa, ib);
   }
   // the step's control fields: loaded now, used once the tile has landed
@@ -499,7 +510,7 @@ __global__ void __launch_bounds__(kThreads32t, 4) k_hydro32p(
     const float *__restrict__ sig, const float *__restrict__ uu, const float *__restrict__ ww,
     const float *__restrict__ Phi, const double *__restrict__ gRin, const double *__restrict__ gpin,
     float *__restrict__ so, float *__restrict__ uo, float *__restrict__ wo, SplitBf16 Sx, Ctl *ctl, Rows32 g,
-    int *rowpend) {
+    int *rowpend, int early_state) {
   extern __shared__ __align__(16) uint8_t sm32p_raw[];
   // TMA destinations: the field offsets are multiples of 128 bytes from a 128-aligned base
   float *sm32t = reinterpret_cast<float *>(((uintptr_t)sm32p_raw + 127) & ~(uintptr_t)127);
@@ -515,10 +526,10 @@ __global__ void __launch_bounds__(kThreads32t, 4) k_hydro32p(
   const int i0 = blockIdx.y * kTileI;
   if (i0 >= 3 && i0 + kTileI + 3 <= g.Nu)
     hydro32p_tile<G2, FM, true>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum, &tmS,
-                                &tmU, &tmW, &tmP, &bar_ld, &bar_rc);
+                                &tmU, &tmW, &tmP, &bar_ld, &bar_rc, early_state != 0);
   else
     hydro32p_tile<G2, FM, false>(sig, uu, ww, Phi, gRin, gpin, so, uo, wo, Sx, ctl, g, sm32t, red, bsum, zsum, &tmS,
-                                 &tmU, &tmW, &tmP, &bar_ld, &bar_rc);
+                                 &tmU, &tmW, &tmP, &bar_ld, &bar_rc, early_state != 0);
   if (rowpend) rowtile_done(rowpend + blockIdx.y);  // this tile's outputs are written
 }
 

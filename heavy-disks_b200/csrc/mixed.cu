@@ -76,11 +76,13 @@ struct MixedState {
   // FP32 field tiles of the packed hydro kernel: sigma, u, w of both ping-pong buffers, dPhi
   CUtensorMap mSig[2], mU[2], mW[2], mPhi;
   // row-tile counters between a step's hydro kernel and the next step's fused phi transform
-  // (dg_common.cuh rowtile_*); zero between steps.  rs_step: the gravity being enqueued is
-  // part of a time step whose hydro signals them.  DISKGPU_ROWSYNC=0 turns the hand-over off
-  // (the phi transform then waits for the whole hydro grid).
+  // (dg_common.cuh rowtile_*); zero between steps.  rs_arm: the gravity being enqueued is
+  // part of a time step whose hydro counts them down (its inverse transform arms them);
+  // rs_wait: its phi transform waits on them, which needs the hydro enqueued just before it
+  // to have counted them down (prev_rs; otherwise it waits for its predecessor kernel).
+  // DISKGPU_ROWSYNC=0 turns the hand-over off.
   int *rowpend = nullptr;
-  bool rs_step = false, rowsync = true;
+  bool rs_arm = false, rs_wait = false, prev_rs = false, rowsync = true;
   bool rowsync_ok() const {
     return rowsync && fused_phi && rowpend && (hydro_kind == kHydroTile || hydro_kind == kHydroPacked);
   }
@@ -877,7 +879,7 @@ static int build_basic(dg_handle *h, const double *Sig, const double *vp) {
 
 static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *u, const float *w, const float *Phi,
                                   const double *gR, const double *gp, int fm, float *so, float *uo, float *wo, Ctl *ctl,
-                                  cudaStream_t st, int *rowpend = nullptr);
+                                  cudaStream_t st, int *rowpend = nullptr, bool early_state = false);
 
 int dg_handle::mixed_upload_state(const double *Sig, const double *vRh, const double *vph) {
   MixedState &X = *mx;
@@ -892,8 +894,6 @@ int dg_handle::mixed_upload_state(const double *Sig, const double *vRh, const do
   XK(cudaMemcpyAsync(VP[0], vph, n * sizeof(double), cudaMemcpyHostToDevice, st));
   k_to_pert<<<grid_for(n), 256, 0, st>>>(S[0], VR[0], VP[0], X.sig[cur], X.u[cur], X.w[cur], X.Sx, X.rows);
   XK(cudaGetLastError());
-  // no hydro step is in flight: the row-tile counters start from zero
-  XK(cudaMemsetAsync(X.rowpend, 0, (size_t)(p.Nu + kTileI - 1) / kTileI * sizeof(int), st));
   if (!in_step_host && !X.tuned) {
     int rc = mixed_autotune();
     if (rc) return rc;
@@ -901,6 +901,12 @@ int dg_handle::mixed_upload_state(const double *Sig, const double *vRh, const do
     k_to_pert<<<grid_for(n), 256, 0, st>>>(S[0], VR[0], VP[0], X.sig[cur], X.u[cur], X.w[cur], X.Sx, X.rows);
     XK(cudaGetLastError());
   }
+  // no hydro step is in flight: the row-tile counters start from zero.  This memset is the
+  // upload's last operation, so the next step's phi transform (which, with the row-tile
+  // hand-over, does not wait on its predecessor kernel) never directly follows the kernel
+  // that wrote its input.
+  XK(cudaMemsetAsync(X.rowpend, 0, (size_t)(p.Nu + kTileI - 1) / kTileI * sizeof(int), st));
+  X.prev_rs = false;
   return DG_OK;
 }
 
@@ -1114,7 +1120,7 @@ __global__ void k_step_finalize(Ctl *ctl) {
 
 static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *u, const float *w, const float *Phi,
                                   const double *gR, const double *gp, int fm, float *so, float *uo, float *wo, Ctl *ctl,
-                                  cudaStream_t st, int *rowpend) {
+                                  cudaStream_t st, int *rowpend, bool early_state) {
   if (X.hydro_kind == MixedState::kHydroPacked) {
     dim3 grid((X.Nphi + kTileJp - 1) / kTileJp, (X.Nu + kTileI - 1) / kTileI);
     const SplitBf16 sx{X.Sx.hi, X.Sx.lo};
@@ -1122,7 +1128,7 @@ static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *
     const int b = (sig == X.sig[1]) ? 1 : 0;  // which ping-pong buffer holds the input
     auto go = [&](auto kern) {
       e = launch_pdl(kern, grid, dim3(kThreads32t), kSmem32p, st, X.mSig[b], X.mU[b], X.mW[b], X.mPhi, sig, u, w, Phi,
-                     gR, gp, so, uo, wo, sx, ctl, X.rows, rowpend);
+                     gR, gp, so, uo, wo, sx, ctl, X.rows, rowpend, early_state ? 1 : 0);
     };
     const bool g2 = X.rows.gamma2 != 0;
     if (fm == kForcePhi) g2 ? go(k_hydro32p<true, kForcePhi>) : go(k_hydro32p<false, kForcePhi>);
@@ -1170,7 +1176,7 @@ int dg_handle::mixed_gravity() {
     if (X.fused_phi) {
       // real 32-point stage, twiddle, complex 32-point stage: 4 rows per CTA
       tc::PhiFwdArgs f{X.Sx.hi, X.Sx.lo, X.twphi, X.Xin.hi, X.Xin.lo, nm * A, Nphi, &ctl->status,
-                       X.rs_step ? X.rowpend : nullptr};
+                       X.rs_wait ? X.rowpend : nullptr};
       XK(launch_pdl(tc::k_phifwd, dim3(Nu / tc::kPfRows), dim3(tc::kPfThreads), tc::kPfSmem, st, X.mPA[0], X.mPA[1],
                     X.mPB[0], X.mPB[1], f));
     } else {
@@ -1204,7 +1210,7 @@ int dg_handle::mixed_gravity() {
     // G4: inverse phi DFT: the fused two-stage kernel from Zt, or a product with Z as an
     // MN-major operand; in a time step it arms the hydro's row-tile counters with the hydro
     // launch's column-tile count
-    int *rp = X.rs_step ? X.rowpend : nullptr;
+    int *rp = X.rs_arm ? X.rowpend : nullptr;
     const int rp_n = (Nu + kTileI - 1) / kTileI;
     const int rp_val =
         X.hydro_kind == MixedState::kHydroPacked ? (Nphi + kTileJp - 1) / kTileJp : (Nphi + kTileJ - 1) / kTileJ;
@@ -1262,16 +1268,20 @@ int dg_handle::mixed_enqueue_step() {
   const bool rs = p.selfgrav && X.rowsync_ok();
   if (p.selfgrav) {
     XK(prof_begin(DG_PROF_GRAVITY));
-    X.rs_step = rs;
+    X.rs_arm = rs;
+    X.rs_wait = rs && X.prev_rs;
     int rc = mixed_gravity();
-    X.rs_step = false;
+    X.rs_arm = X.rs_wait = false;
     if (rc) return rc;
     XK(prof_end(DG_PROF_GRAVITY));
     fm = kForcePhi;
   }
   XK(prof_begin(DG_PROF_HYDRO));
+  // with self-gravity the hydro's predecessor is the inverse phi transform, which writes
+  // only dPhi: the packed form may fetch the state before its dependence wait
   XK(launch_hydro32(X, X.sig[c], X.u[c], X.w[c], X.dPhi, nullptr, nullptr, fm, X.sig[o], X.u[o], X.w[o], ctl, st,
-                    rs ? X.rowpend : nullptr));
+                    rs ? X.rowpend : nullptr, fm == kForcePhi));
+  X.prev_rs = rs;
   XK(prof_end(DG_PROF_HYDRO));
   cur = o;
   return DG_OK;
@@ -1303,6 +1313,7 @@ int dg_handle::mixed_enqueue_step_forces(const double *gRh, const double *gph) {
     fm = kForceArrays;
   }
   const int c = cur, o = cur ^ 1;
+  X.prev_rs = false;
   XK(launch_hydro32(X, X.sig[c], X.u[c], X.w[c], nullptr, gA, gB, fm, X.sig[o], X.u[o], X.w[o], ctl, st));
   cur = o;
   return DG_OK;
