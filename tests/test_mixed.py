@@ -164,3 +164,27 @@ def test_autotuner_reports_its_choice(monkeypatch):
         assert c.tuning().startswith("tuning off")
         assert c.timestep(0.3) == dt_tuned
         np.testing.assert_array_equal(c.get_state()[0], S_tuned)
+
+
+def test_row_tile_handover_is_bit_identical(monkeypatch):
+    """The row-tile hand-over between a step's hydro kernel and the next step's phi
+    transform (on by default at 1024^2) changes only when kernels may start, never what
+    they compute: the state after graph-launched steps, a caller-forces step and single
+    steps is bit-for-bit the one with the hand-over off (DISKGPU_ROWSYNC=0)."""
+    monkeypatch.delenv("DISKGPU_HYDRO32", raising=False)
+    out = []
+    for rs in ("1", "0"):
+        monkeypatch.setenv("DISKGPU_ROWSYNC", rs)
+        with D.Disk(1024, 1024, eps=0.005, amp=1e-2, precision="mixed") as d:
+            d.init_standard()
+            d.run_steps(40, 0.3)
+            dt = d.timestep(0.3)
+            d.step_forces(dt)        # hydro with the disk's own gravity switched off
+            d.step(dt)               # single self-gravity steps right after it
+            d.step(dt)
+            d.run_steps(24, 0.3)
+            out.append((d.get_state(), d.time()))
+    (a, ta), (b, tb) = out
+    assert ta == tb
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
