@@ -115,6 +115,12 @@ __device__ __forceinline__ void hydro32p_tile(
   const bool outx = lane >= 2 && lane <= 30 && xs0 + 2 * lane <= Nphi;
   const bool outy = lane >= 1 && lane <= 29 && xs0 + 2 * lane + 1 <= Nphi;
 #define RC(k, i) rc[((i) - ib) * kRowTabW + (k)]
+  // four row constants of row i in one shared-memory broadcast (rows are 80-byte aligned)
+#define RC4(b, i) (*reinterpret_cast<const float4 *>(rc + ((i) - ib) * kRowTabW + 4 * (b)))
+  static_assert(tS0 == 0 && tInvS0 == 1 && tV0 == 2 && tA0 == 3 && tDP0 == 4 && tInvdRc == 5 && tInvR == 6 &&
+                    tR == 7 && tInvVol == 8 && tInvdl == 9 && tAphi == 10 && tR32 == 11 && tInvdR == 12 &&
+                    tDS0 == 14 && tDV == 15 && tAf == 16 && tInvdRl == 17 && tInvdRr == 18,
+                "the float4 groups of the row-constant loads below");
   auto row_ok = [&](int i) { return IN || (i >= 0 && i < Nu); };
   auto first_row = [&](int i) { return !IN && i == 0; };
   auto last_row = [&](int i) { return !IN && i == Nu - 1; };
@@ -253,13 +259,14 @@ __device__ __forceinline__ void hydro32p_tile(
       }
       F2 nu1 = S(0.f), nw1 = S(0.f);
       if (row_ok(i)) {
+        const float4 c0 = RC4(0, i), c1 = RC4(1, i);  // S0 invS0 V0 a0 | dP0/dR invdRc invR R
         const F2 s_g = SG[x];
-        const F2 s = add(S(RC(tS0, i)), s_g);
+        const F2 s = add(S(c0.x), s_g);
         const F2 pim = first_row(i) ? dc : DP[x - L2];
         const F2 pip = last_row(i) ? dc : DP[x + L2];
-        const F2 ddP = mul(sub(pip, pim), S(RC(tInvdRc, i)));
+        const F2 ddP = mul(sub(pip, pim), S(c1.y));
         const F2 dPdphi = mul(sub(make_float2(dc.y, dr), make_float2(dl, dc.x)), S(g.inv2dphi));
-        const float iR = RC(tInvR, i);
+        const float iR = c1.z;
         F2 dgR = S(0.f), dgp = S(0.f);
         if (FM == kForcePhi) {
           F2 dPhidu;
@@ -274,10 +281,10 @@ __device__ __forceinline__ void hydro32p_tile(
           dgp = make_float2((float)gpin[q], (float)gpin[q + 1]);
         }
         const F2 uc = U0[x], wc = W0[x];  // raw u, w of the point (row r of the staged fields)
-        const float V = RC(tV0, i);
-        const F2 q1 = fdiv(sub(mul(mul(S(RC(tDP0, i)), s_g), S(RC(tInvS0, i))), ddP), s);
-        const F2 aR = add(add(add(S(RC(tA0, i)), q1), dgR), mul(mul(add(S(2.f * V), wc), wc), S(iR)));
-        const F2 q2 = fdiv(mul(dPdphi, S(-1.f)), mul(s, S(RC(tR, i))));
+        const float V = c0.z;
+        const F2 q1 = fdiv(sub(mul(mul(S(c1.x), s_g), S(c0.y)), ddP), s);
+        const F2 aR = add(add(add(S(c0.w), q1), dgR), mul(mul(add(S(2.f * V), wc), wc), S(iR)));
+        const F2 q2 = fdiv(mul(dPdphi, S(-1.f)), mul(s, S(c1.w)));
         const F2 ap = sub(add(q2, dgp), mul(mul(uc, add(S(V), wc)), S(iR)));
         nu1 = fma(S(dt), aR, uc);
         nw1 = fma(S(dt), ap, wc);
@@ -303,15 +310,17 @@ __device__ __forceinline__ void hydro32p_tile(
         const F2 vf = mul(S(0.5f), add(u1, u2));
         const bool ux = vf.x > 0.f, uy = vf.y > 0.f;
         const F2 vdt = mul(vf, S(dt));
-        const F2 hu = mul(S(0.5f), sub(S(1.f), mul(vdt, S(RC(tInvdRl, f)))));
-        const F2 hd = mul(S(-0.5f), add(S(1.f), mul(vdt, S(RC(tInvdRr, f)))));
+        // face constants: DS0 / DV of faces f-1, f, f+1; Af, invdRl, invdRr of face f
+        const float4 cm = RC4(3, f - 1), cf = RC4(3, f), cp = RC4(3, f + 1), ca = RC4(4, f);
+        const F2 hu = mul(S(0.5f), sub(S(1.f), mul(vdt, S(ca.y))));
+        const F2 hd = mul(S(-0.5f), add(S(1.f), mul(vdt, S(ca.z))));
         const F2 hf = sel(ux, uy, hu, hd);
         // cells cc-1, cc, cc+1 with cc = f-1 (upwind from below) or f
         const F2 sa = sel(ux, uy, s0, s1), sb = sel(ux, uy, s1, s2), sc = sel(ux, uy, s2, s3);
         const F2 ua = sel(ux, uy, u0, u1), ub = sel(ux, uy, u1, u2), uc = sel(ux, uy, u2, u3);
         const F2 wa = sel(ux, uy, w0, w1), wb = sel(ux, uy, w1, w2), wc = sel(ux, uy, w2, w3);
-        const F2 ds_c = sels(ux, uy, RC(tDS0, f - 1), RC(tDS0, f)), ds_c1 = sels(ux, uy, RC(tDS0, f), RC(tDS0, f + 1));
-        const F2 dv_c = sels(ux, uy, RC(tDV, f - 1), RC(tDV, f)), dv_c1 = sels(ux, uy, RC(tDV, f), RC(tDV, f + 1));
+        const F2 ds_c = sels(ux, uy, cm.z, cf.z), ds_c1 = sels(ux, uy, cf.z, cp.z);
+        const F2 dv_c = sels(ux, uy, cm.w, cf.w), dv_c1 = sels(ux, uy, cf.w, cp.w);
         const F2 s0_c = sels(ux, uy, RC(tS0, f - 1), RC(tS0, f));
         F2 kS = vanleer(add(ds_c1, sub(sc, sb)), add(ds_c, sub(sb, sa)));
         F2 kU = vanleer(sub(uc, ub), sub(ub, ua));
@@ -325,9 +334,9 @@ __device__ __forceinline__ void hydro32p_tile(
         }
         const F2 Sf = fma(hf, kS, add(s0_c, sb));
         const F2 uf = fma(hf, kU, ub);
-        const float dVf = RC(tDV, f);
+        const float dVf = cf.w;
         const F2 Df = fma(hf, kV, add(sels(ux, uy, 0.f, dVf), wb));  // vphi_f - V0(f-1)
-        F = mul(mul(vf, Sf), S(RC(tAf, f)));
+        F = mul(mul(vf, Sf), S(ca.x));
         FRv = mul(F, uf);
         GAv = mul(F, Df);
         GBv = mul(F, sub(Df, S(dVf)));
@@ -370,7 +379,8 @@ __device__ __forceinline__ void hydro32p_tile(
       const float sL0 = up1(sm.x), sL1 = up1(sm.y), sR = dn1(sm.x);
       const float uL0 = up1(um.x), uL1 = up1(um.y), uR = dn1(um.x);
       const float wL0 = up1(wm.x), wL1 = up1(wm.y), wR = dn1(wm.x);
-      const float V = RC(tV0, i), idl = RC(tInvdl, i), S0 = RC(tS0, i), A = RC(tAphi, i);
+      const float4 c0 = RC4(0, i), c2 = RC4(2, i);  // S0 invS0 V0 a0 | invVol invdl Aphi R32
+      const float V = c0.z, idl = c2.y, S0 = c0.x, A = c2.z;
       const F2 dv = mul(S(0.5f), add(make_float2(wL1, wm.x), make_float2(wm.x, wm.y)));
       const F2 vf = add(S(V), dv);
       const bool ux = vf.x > 0.f, uy = vf.y > 0.f;
@@ -407,7 +417,8 @@ __device__ __forceinline__ void hydro32p_tile(
       // right face of column 2l+1 is the right lane's first face
       const F2 fm1 = make_float2(fm.y, dn1(fm.x)), fr1 = make_float2(fr.y, dn1(fr.x)), fg1 = make_float2(fg.y, dn1(fg.x));
       if (outx || outy) {
-        const float iv = RC(tInvVol, i), S0 = RC(tS0, i);
+        const float4 c0 = RC4(0, i), c2 = RC4(2, i);  // S0 invS0 V0 a0 | invVol invdl Aphi R32
+        const float iv = c2.x, S0 = c0.x;
         const F2 s2 = SG[x], u2 = U2[x], w2 = W2[x];
         const F2 sn2 = add(S(S0), s2);
         F2 s3 = fma(mul(S(dt), sub(fm, fm1)), S(iv), s2);
@@ -418,7 +429,7 @@ __device__ __forceinline__ void hydro32p_tile(
         const F2 w3 = fdiv(fma(mul(S(dt), sub(fg, fg1)), S(iv), mul(sn2, w2)), d);
         s3 = make_float2(flx ? 1e-10f - S0 : s3.x, fly ? 1e-10f - S0 : s3.y);
         const size_t q = (size_t)i * Nphi + jc;
-        const float R32 = RC(tR32, i);
+        const float R32 = c2.w;
         const F2 xr = mul(S(R32), s3);
         // split-BF16 operand: one packed conversion per plane, the roundings of split_bf16
         const __nv_bfloat162 h2 = __floats2bfloat162_rn(xr.x, xr.y);
@@ -444,7 +455,7 @@ __device__ __forceinline__ void hydro32p_tile(
         const float gk = g.gamma * g.Kpoly;
         const F2 cs = G2 ? make_float2(sqrtf(gk * scl.x), sqrtf(gk * scl.y))
                          : make_float2(sqrtf(gk * powf(scl.x, g.gamma - 1.f)), sqrtf(gk * powf(scl.y, g.gamma - 1.f)));
-        const float V = RC(tV0, i), idR = RC(tInvdR, i), idl = RC(tInvdl, i);
+        const float V = c0.z, idR = RC(tInvdR, i), idl = c2.y;
         const F2 rate = fma(add(make_float2(fabsf(V + w3.x), fabsf(V + w3.y)), cs), S(idl),
                             mul(add(make_float2(fabsf(u3.x), fabsf(u3.y)), cs), S(idR)));
         if (outx) {
