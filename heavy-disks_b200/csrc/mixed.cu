@@ -879,7 +879,9 @@ static int build_basic(dg_handle *h, const double *Sig, const double *vp) {
 
 static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *u, const float *w, const float *Phi,
                                   const double *gR, const double *gp, int fm, float *so, float *uo, float *wo, Ctl *ctl,
-                                  cudaStream_t st, int *rowpend = nullptr, bool early_state = false);
+                                  cudaStream_t st, int *rowpend = nullptr, bool early_state = false,
+                                  bool finalize = true);
+static cudaError_t launch_finalize(const MixedState &X, Ctl *ctl, cudaStream_t st);
 
 int dg_handle::mixed_upload_state(const double *Sig, const double *vRh, const double *vph) {
   MixedState &X = *mx;
@@ -1118,9 +1120,15 @@ __global__ void k_step_finalize(Ctl *ctl) {
   if (threadIdx.x == 0) finalize_launch(ctl, read_step_info(ctl, true, ctl->pend_active));
 }
 
+// the step's finalisation after a tile hydro launch (the warp form finalises in its last CTA)
+static cudaError_t launch_finalize(const MixedState &X, Ctl *ctl, cudaStream_t st) {
+  if (X.hydro_kind == MixedState::kHydroWarp) return cudaSuccess;
+  return launch_pdl(k_step_finalize, dim3(1), dim3(32), 0, st, ctl);
+}
+
 static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *u, const float *w, const float *Phi,
                                   const double *gR, const double *gp, int fm, float *so, float *uo, float *wo, Ctl *ctl,
-                                  cudaStream_t st, int *rowpend, bool early_state) {
+                                  cudaStream_t st, int *rowpend, bool early_state, bool finalize) {
   if (X.hydro_kind == MixedState::kHydroPacked) {
     dim3 grid((X.Nphi + kTileJp - 1) / kTileJp, (X.Nu + kTileI - 1) / kTileI);
     const SplitBf16 sx{X.Sx.hi, X.Sx.lo};
@@ -1134,7 +1142,7 @@ static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *
     if (fm == kForcePhi) g2 ? go(k_hydro32p<true, kForcePhi>) : go(k_hydro32p<false, kForcePhi>);
     else if (fm == kForceArrays) g2 ? go(k_hydro32p<true, kForceArrays>) : go(k_hydro32p<false, kForceArrays>);
     else g2 ? go(k_hydro32p<true, kForceNone>) : go(k_hydro32p<false, kForceNone>);
-    if (e == cudaSuccess) e = launch_pdl(k_step_finalize, dim3(1), dim3(32), 0, st, ctl);
+    if (e == cudaSuccess && finalize) e = launch_finalize(X, ctl, st);
     return e;
   }
   if (X.hydro_kind == MixedState::kHydroTile) {
@@ -1149,7 +1157,7 @@ static cudaError_t launch_hydro32(MixedState &X, const float *sig, const float *
     if (fm == kForcePhi) g2 ? go(k_hydro32t<true, kForcePhi>) : go(k_hydro32t<false, kForcePhi>);
     else if (fm == kForceArrays) g2 ? go(k_hydro32t<true, kForceArrays>) : go(k_hydro32t<false, kForceArrays>);
     else g2 ? go(k_hydro32t<true, kForceNone>) : go(k_hydro32t<false, kForceNone>);
-    if (e == cudaSuccess) e = launch_pdl(k_step_finalize, dim3(1), dim3(32), 0, st, ctl);
+    if (e == cudaSuccess && finalize) e = launch_finalize(X, ctl, st);
     return e;
   }
   if (rowpend) return cudaErrorInvalidValue;  // the warp form has no row-tile hand-over
@@ -1280,9 +1288,10 @@ int dg_handle::mixed_enqueue_step() {
   // with self-gravity the hydro's predecessor is the inverse phi transform, which writes
   // only dPhi: the packed form may fetch the state before its dependence wait
   XK(launch_hydro32(X, X.sig[c], X.u[c], X.w[c], X.dPhi, nullptr, nullptr, fm, X.sig[o], X.u[o], X.w[o], ctl, st,
-                    rs ? X.rowpend : nullptr, fm == kForcePhi));
+                    rs ? X.rowpend : nullptr, fm == kForcePhi, false));
   X.prev_rs = rs;
-  XK(prof_end(DG_PROF_HYDRO));
+  XK(prof_end(DG_PROF_HYDRO));  // the hydro kernel alone; its finalisation follows
+  XK(launch_finalize(X, ctl, st));
   cur = o;
   return DG_OK;
 }
