@@ -1,7 +1,7 @@
 """ctypes binding of the plain-C oracle (liboracle.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by the
-CPU-baseline leg of bench.py, as the checker.  Nothing in the product imports it.
+CPU-baseline leg of bench.py, to check results against.  Nothing in the product imports it.
 It restates diskfft/src/{hydro.hpp,kalnajs.hpp,diskmain.cpp}; see diskoracle.h.
 """
 from __future__ import annotations

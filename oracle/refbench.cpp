@@ -1,4 +1,4 @@
-// refbench — times the reference's own time step on the host cores.  TEST / BASELINE
+// refbench — times the reference's own time step on the host cores.  TEST AND CPU-BASELINE
 // INFRASTRUCTURE ONLY.  It drives diskfft/src/hydro.hpp and diskfft/src/kalnajs.hpp
 // (compiled unmodified against the FFTW shim) through the loop body of
 // diskfft/src/diskmain.cpp:100-109: timestep(0.3) -> potential -> forces -> step, and

@@ -4,7 +4,8 @@ DFT gravity) against the FP64 oracle.
 Tolerances (stated per check): the split-BF16 products carry ~2^-16 relative error per
 term, so the gravity of a field agrees with the FP64 potential to <= 2e-4 relative; the
 perturbation fields after 100 steps agree to <= 2e-3 of the perturbation's own size;
-gamma and Omega_p from the same run agree to <= 0.5 %."""
+gamma and Omega_p from the same run agree to <= 0.5 % (the mixed path's accuracy
+requirement)."""
 import numpy as np
 import pytest
 

@@ -1,7 +1,7 @@
 """Plain-method (FP64) GPU path against the reference (golden fixtures from the
-reference build) and against the oracle at larger sizes.  Tolerance: the north-star
-bar of <= 1e-10 relative in Sigma, vR, vphi after 100 steps; observed errors are
-round-off (~1e-14)."""
+reference build) and against the oracle at larger sizes.  Tolerance: <= 1e-10 relative
+in Sigma, vR, vphi after 100 steps (the plain path's accuracy requirement); observed
+errors are round-off (~1e-14)."""
 import os
 import subprocess
 
@@ -67,7 +67,7 @@ def test_known_answer_fft_vs_direct_on_gpu():
 
 @pytest.mark.parametrize("N,steps", [(256, 100), (128, 100), (384, 20), (1024, 4)])
 def test_fp64_vs_oracle_after_steps(N, steps):
-    """configs[0] grid (256^2, eps 0.005) for 100 steps, plus other sizes."""
+    """The reference's CPU-runnable case (256^2, eps 0.005) for 100 steps, plus other sizes."""
     kw = dict(Nu=N, Nphi=N, eps=0.005, amp=1e-3)
     ref = O.Disk(nthreads=8, **kw)
     with D.Disk(N, N, eps=0.005, amp=1e-3) as d:
