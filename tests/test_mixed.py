@@ -56,8 +56,11 @@ def test_state_roundtrip_mixed():
         assert m == pytest.approx(ref.mD, rel=1e-12)
 
 
-@pytest.mark.parametrize("N,steps", [(256, 100), (128, 200)])
+@pytest.mark.parametrize("N,steps", [(256, 100), (128, 200), (1024, 50)])
 def test_mixed_vs_fp64_after_steps(N, steps):
+    """Mixed-path fields after the given steps (dt from the oracle's CFL, checked against the
+    device's) against the FP64 oracle stepped in lockstep; 1024^2 runs the fused transforms
+    and the packed hydro."""
     ref = O.Disk(Nu=N, Nphi=N, eps=0.005, amp=1e-3, nthreads=8)
     S0 = ref.hyd.get("Sig").mean(axis=1, keepdims=True)
     with D.Disk(N, N, eps=0.005, amp=1e-3, precision="mixed") as d:
