@@ -5,7 +5,10 @@
 // The initial condition and loop body restate diskfft/src/diskmain.cpp:28-63 and
 // :100-109 (timestep 0.3 -> potential -> forces -> step), without the tlim clip.
 //
-// usage: refdump Nu Nphi eps selfgrav amp nsteps out.bin [nthreads]
+// usage: refdump Nu Nphi eps selfgrav amp nsteps out.bin [nthreads [gamma_gas Kpoly S0]]
+// The optional physics arguments replace the constants of diskmain.cpp:28-29 (the
+// reference's DiskHydro takes K and Gamma as constructor arguments, hydro.hpp:28), so
+// fixtures can pin the general-Gamma pressure and sound-speed branches (hydro.hpp:45-46).
 // out.bin: int32 Nu, Nphi, nsteps, selfgrav; float64 eps, amp, mD; then float64 arrays
 //   Sig0 vR0 vp0 Phi0 gR0 gp0 (Nu*Nphi each, initial state and its gravity),
 //   dt[nsteps], SigN vRN vpN, c0 ph0 c2 ph2 (modes of the final state).
@@ -24,7 +27,10 @@ using namespace diskfft;
 static void wr(FILE *f, const std::vector<double> &v) { fwrite(v.data(), sizeof(double), v.size(), f); }
 
 int main(int argc, char **argv) {
-  if (argc < 8) { fprintf(stderr, "usage: refdump Nu Nphi eps selfgrav amp nsteps out.bin [nthreads]\n"); return 2; }
+  if (argc < 8) {
+    fprintf(stderr, "usage: refdump Nu Nphi eps selfgrav amp nsteps out.bin [nthreads [gamma_gas Kpoly S0]]\n");
+    return 2;
+  }
   int Nu = atoi(argv[1]), Nphi = atoi(argv[2]);
   double eps = atof(argv[3]);
   int selfgrav = atoi(argv[4]);
@@ -36,6 +42,11 @@ int main(int argc, char **argv) {
 #endif
   double Rin = 0.25, Rout = 1.0, R0 = 0.45, w2 = 0.05, S0 = 0.372;
   double Kpoly = 0.25, gamma_gas = 2.0, gmstar = 0.6, G = 1.0;
+  if (argc > 11) {
+    gamma_gas = atof(argv[9]);
+    Kpoly = atof(argv[10]);
+    S0 = atof(argv[11]);
+  }
   DiskHydro hyd(Nu, Nphi, Rin, Rout, Kpoly, gamma_gas, gmstar);
   KalnajsSolver grav(Nu, Nphi, Rin, Rout, eps, G, nthreads);
   auto Sigma0 = [&](double R) { return S0 * std::exp(-(R - R0) * (R - R0) / w2); };

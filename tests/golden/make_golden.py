@@ -34,7 +34,19 @@ CASES = {
     "64x64_strong": (64, 64, 0.005, 1, 0.2, 40),
     "8x12_sg": (8, 12, 0.04, 1, 0.1, 25),
     "24x27_odd": (24, 27, 0.02, 1, 0.1, 12),
+    # general-Gamma disks of the sweep law (hydro.hpp:45-46 with Gamma != 2): the physics
+    # of two sweep points, as dg_params_physical maps (Q_min, M_d/M_*, softening/r, Gamma)
+    # (1.1, 0.3, 0.15, 1.5) and (1.6, 0.8, 0.07, 1.75); the second has its K capped
+    "40x48_g1.5": (40, 48, 0.0225, 1, 5e-2, 20),
+    "32x40_g1.75": (32, 40, 0.0049, 1, 0.1, 20),
 }
+
+# name: (gamma_gas, Kpoly, S0) for the cases whose physics differs from diskmain.cpp:28-29
+PHYSICS = {
+    "40x48_g1.5": (1.5, 0.08770103346609004, 0.16741633318186389),
+    "32x40_g1.75": (1.75, 0.1975331689842986, 0.44644355515163703),
+}
+STANDARD_PHYSICS = (2.0, 0.25, 0.372)
 
 DISKDISK = {
     # name: argv of diskdisk (Nu Nphi eps tlim selfgrav amp nthreads)
@@ -61,9 +73,12 @@ def main():
         if not want(name):
             continue
         out = os.path.join(tmp, name + ".bin")
+        phys = PHYSICS.get(name, STANDARD_PHYSICS)
+        extra = ["1"] + [repr(x) for x in phys] if name in PHYSICS else []
         subprocess.run([os.path.join(ref, "refdump"), str(Nu), str(Nphi), repr(eps), str(sg),
-                        repr(amp), str(n), out], check=True)
+                        repr(amp), str(n), out] + extra, check=True)
         r = O.read_refdump(out)
+        r["gamma_gas"], r["Kpoly"], r["S0"] = phys
         np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"), **{k: np.asarray(v) for k, v in r.items()})
     if want("test_kalnajs_ref"):
         res = subprocess.run([os.path.join(ref, "test_kalnajs_ref")], capture_output=True, text=True)

@@ -16,6 +16,13 @@ def rel_err(a, b):
     return float(np.max(np.abs(a - b))) / den
 
 
+def golden_physics(g):
+    """(gamma_gas, Kpoly, S0) of a golden case; the standard disk (diskmain.cpp:28-29) when
+    the fixture does not carry them."""
+    return (float(g["gamma_gas"]) if "gamma_gas" in g else 2.0, float(g["Kpoly"]) if "Kpoly" in g else 0.25,
+            float(g["S0"]) if "S0" in g else 0.372)
+
+
 def golden_cases():
     out = {}
     for f in sorted(glob.glob(os.path.join(GOLDEN, "ref_*.npz"))):

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from helpers import GOLDEN, golden_cases, rel_err
+from helpers import GOLDEN, golden_cases, golden_physics, rel_err
 
 CASES = golden_cases()
 
@@ -24,7 +24,9 @@ def _built():
 def test_restatement_matches_reference_bitwise(name):
     g = CASES[name]
     Nu, Nphi = int(g["Nu"]), int(g["Nphi"])
-    d = O.Disk(Nu=Nu, Nphi=Nphi, eps=float(g["eps"]), selfgrav=int(g["selfgrav"]), amp=float(g["amp"]))
+    gam, K, S0 = golden_physics(g)
+    d = O.Disk(Nu=Nu, Nphi=Nphi, eps=float(g["eps"]), selfgrav=int(g["selfgrav"]), amp=float(g["amp"]),
+               gamma_gas=gam, Kpoly=K, S0=S0)
     S, vR, vp = d.hyd.state()
     assert np.array_equal(S, g["Sig0"]) and np.array_equal(vR, g["vR0"]) and np.array_equal(vp, g["vp0"])
     Phi = d.grav.potential(S)

@@ -10,7 +10,7 @@ import pytest
 
 import diskgpu as D
 import oracle as O
-from helpers import GOLDEN, ROOT, golden_cases, rel_err
+from helpers import GOLDEN, ROOT, golden_cases, golden_physics, rel_err
 
 pytestmark = pytest.mark.gpu
 CASES = golden_cases()
@@ -18,8 +18,9 @@ TOL = 1e-10
 
 
 def _disk(g, **kw):
+    gam, K, S0 = golden_physics(g)
     return D.Disk(int(g["Nu"]), int(g["Nphi"]), eps=float(g["eps"]), selfgrav=int(g["selfgrav"]),
-                  amp=float(g["amp"]), **kw)
+                  amp=float(g["amp"]), gamma_gas=gam, Kpoly=K, S0=S0, **kw)
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
