@@ -366,22 +366,37 @@ int dg_handle::download_state(double *Sig, double *vRh, double *vph) {
 // ---------------------------------------------------------------------------------
 // chunked loop: a CUDA graph holds kGraphSteps steps (an even count, so it starts and
 // ends on the same ping-pong buffer).
+// Record kGraphSteps steps into graph_exec (nothing runs: a capture only records).
+int dg_handle::capture_graph() {
+  if (graph_exec || !use_graphs) return DG_OK;
+  if (cur != 0) return fail(DG_ERR_STATE, "dg_capture_graph", "the state sits in the second ping-pong buffer");
+  cudaGraph_t g = nullptr;
+  // enqueue_step keeps host-side flags of what the last enqueued kernels were; recording
+  // runs nothing, so they are put back, and a launch of the graph applies their end values
+  const int flags_before = loop_flags();
+  MK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  int rc = DG_OK;
+  for (int k = 0; k < kGraphSteps && !rc; ++k) rc = enqueue_step();
+  cudaError_t e = cudaStreamEndCapture(st, &g);
+  graph_end_flags = loop_flags();
+  set_loop_flags(flags_before);
+  cur = 0;  // enqueue_step flipped cur kGraphSteps times during capture
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  MK(e);
+  e = cudaGraphInstantiate(&graph_exec, g, 0);
+  cudaGraphDestroy(g);
+  MK(e);
+  return DG_OK;
+}
+
 int dg_handle::run_chunk(int nsteps) {
   if (nsteps == kGraphSteps && cur == 0 && use_graphs && !prof_on) {
     if (!graph_exec) {
-      cudaGraph_t g = nullptr;
-      MK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      int rc = DG_OK;
-      for (int k = 0; k < kGraphSteps && !rc; ++k) rc = enqueue_step();
-      cudaError_t e = cudaStreamEndCapture(st, &g);
-      if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-      MK(e);
-      e = cudaGraphInstantiate(&graph_exec, g, 0);
-      cudaGraphDestroy(g);
-      MK(e);
-      cur = 0;  // enqueue_step flipped cur kGraphSteps times during capture
+      int rc = capture_graph();
+      if (rc) return rc;
     }
     MK(cudaGraphLaunch(graph_exec, st));
+    set_loop_flags(graph_end_flags);
     return DG_OK;
   }
   for (int k = 0; k < nsteps; ++k) {
@@ -411,6 +426,14 @@ int dg_params_default(dg_params *p) {
 }
 
 static thread_local std::string g_create_error;
+
+}  // extern "C"
+
+// Handle-less calls (dg_create, the fits, the parameter file) leave their reason here; it
+// is what dg_last_error(NULL) returns on the same thread.
+void dg_set_global_error(const std::string &why) { g_create_error = why; }
+
+extern "C" {
 
 int dg_create(const dg_params *p, dg_handle **out) {
   if (!p || !out) return DG_ERR_INVALID;
@@ -661,13 +684,16 @@ int dg_time(dg_handle *h, double *t, long long *nsteps) {
   return DG_OK;
 }
 
-int dg_advance(dg_handle *h, double tlim, double cfl, double dtout, dg_record *rec, int max_rec, int *n_rec,
-               double *t_out, long long *nsteps_out) {
-  if (!h || (max_rec > 0 && !rec) || !(cfl > 0) || !(dtout > 0)) return DG_ERR_INVALID;
+}  // extern "C"
+
+// The loop of diskmain.cpp:88-110 on the device, handing every mode record to `sink` in
+// order as soon as the host drains it (after each chunk of steps).
+template <typename Sink>
+static int advance_records(dg_handle *h, double tlim, double cfl, double dtout, Sink &&sink, double *t_out,
+                           long long *nsteps_out) {
   { int rc0 = h->sync_from_device(); if (rc0) return rc0; }
   if (!h->have_state) return h->fail(DG_ERR_STATE, "dg_advance", "no state set");
   DG_CK(cudaSetDevice(h->dev));
-  int nout = 0;
   // diskmain.cpp:88,93: tnext starts at 0 with the state and persists across calls
   int rc = h->set_ctl_fields(h->t, tlim, cfl, 0.0, h->tnext, dtout, 0);
   if (rc) return rc;
@@ -687,13 +713,8 @@ int dg_advance(dg_handle *h, double tlim, double cfl, double dtout, dg_record *r
       DG_CK(cudaMemsetAsync(&h->ctl->nrec, 0, sizeof(int), h->st));
       DG_CK(cudaStreamSynchronize(h->st));
       for (int k = 0; k < nr; ++k) {
-        if (nout < max_rec) {
-          rec[nout].t = tmp[4 * k];
-          rec[nout].c0 = tmp[4 * k + 1];
-          rec[nout].c2 = tmp[4 * k + 2];
-          rec[nout].arg2 = tmp[4 * k + 3];
-        }
-        ++nout;
+        const dg_record r{tmp[4 * k], tmp[4 * k + 1], tmp[4 * k + 2], tmp[4 * k + 3]};
+        sink(r);
       }
     }
     h->t = h->hctl->t;
@@ -711,10 +732,49 @@ int dg_advance(dg_handle *h, double tlim, double cfl, double dtout, dg_record *r
     if (rc) return rc;
   }
   h->tnext = h->hctl->tnext;
-  if (n_rec) *n_rec = nout < max_rec ? nout : max_rec;
   if (t_out) *t_out = h->t;
   if (nsteps_out) *nsteps_out = h->nsteps;
   return DG_OK;
+}
+
+extern "C" {
+
+int dg_advance(dg_handle *h, double tlim, double cfl, double dtout, dg_record *rec, int max_rec, int *n_rec,
+               double *t_out, long long *nsteps_out) {
+  if (!h || (max_rec > 0 && !rec) || !(cfl > 0) || !(dtout > 0)) return DG_ERR_INVALID;
+  int nout = 0;
+  int rc = advance_records(
+      h, tlim, cfl, dtout,
+      [&](const dg_record &r) {
+        if (nout < max_rec) rec[nout] = r;
+        ++nout;
+      },
+      t_out, nsteps_out);
+  if (rc) return rc;
+  if (n_rec) *n_rec = nout < max_rec ? nout : max_rec;
+  return DG_OK;
+}
+
+int dg_advance_cb(dg_handle *h, double tlim, double cfl, double dtout, dg_record_fn fn, void *user, int *n_rec,
+                  double *t_out, long long *nsteps_out) {
+  if (!h || !fn || !(cfl > 0) || !(dtout > 0)) return DG_ERR_INVALID;
+  int nout = 0;
+  int rc = advance_records(
+      h, tlim, cfl, dtout,
+      [&](const dg_record &r) {
+        fn(&r, user);
+        ++nout;
+      },
+      t_out, nsteps_out);
+  if (n_rec) *n_rec = nout;
+  return rc;
+}
+
+int dg_capture_graph(dg_handle *h) {
+  if (!h) return DG_ERR_INVALID;
+  if (!h->have_state) return h->fail(DG_ERR_STATE, "dg_capture_graph", "no state set");
+  DG_CK(cudaSetDevice(h->dev));
+  return h->capture_graph();
 }
 
 int dg_set_stream(dg_handle *h, void *stream) {

@@ -80,6 +80,11 @@ struct dg_handle {
   int modes_launch(int nmodes, double *out);
   int conserved_launch(double *out2);
   int run_chunk(int nsteps);
+  int capture_graph();
+  // host-side state of the enqueued step sequence (the mixed path's row-tile hand-over)
+  int graph_end_flags = 0;
+  int loop_flags() const;
+  void set_loop_flags(int f);
   int upload_state(const double *Sig, const double *vR, const double *vp);
   int download_state(double *Sig, double *vR, double *vp);
 

@@ -63,7 +63,10 @@ EXPORTS = (
     "dg_batch_init_standard", "dg_batch_advance", "dg_save", "dg_load", "dg_set_diagnostics",
     "dg_diagnostics_read", "dg_mlp_create", "dg_mlp_destroy", "dg_mlp_last_error", "dg_mlp_num_params",
     "dg_mlp_get_params", "dg_mlp_set_params", "dg_mlp_forward", "dg_mlp_loss_grad", "dg_mlp_train_step",
+    "dg_capture_graph", "dg_advance_cb", "dg_fit_growth", "dg_fit_phases", "dg_params_write", "dg_params_read",
 )
+
+RECORD_FN = C.CFUNCTYPE(None, C.POINTER(Record), C.c_void_p)
 
 BASIC_FFT, BASIC_ELLIPTIC = 0, 1
 
@@ -144,6 +147,13 @@ def lib():
     L.dg_mlp_forward.argtypes = [H, C.c_int, Fp, Fp]
     L.dg_mlp_loss_grad.argtypes = [H, C.c_int, Fp, Fp, Fp, Fp]
     L.dg_mlp_train_step.argtypes = [H, C.c_int, Fp, Fp, C.c_float, Fp]
+    L.dg_capture_graph.argtypes = [H]
+    L.dg_advance_cb.argtypes = [H, C.c_double, C.c_double, C.c_double, RECORD_FN, C.c_void_p, C.POINTER(C.c_int), D,
+                                C.POINTER(C.c_longlong)]
+    L.dg_fit_growth.argtypes = [C.POINTER(Record), C.c_int, C.c_double, C.c_double, D, D, C.POINTER(C.c_int)]
+    L.dg_fit_phases.argtypes = [C.POINTER(Record), C.c_int, C.c_double, C.c_double, C.c_double, D]
+    L.dg_params_write.argtypes = [C.c_char_p, C.POINTER(Params), C.c_int]
+    L.dg_params_read.argtypes = [C.c_char_p, C.POINTER(Params), C.c_int, C.POINTER(C.c_int)]
     L.dg_timestep_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double,
                                      C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     _lib = L
@@ -193,6 +203,56 @@ def params_physical(Qmin, mass_ratio, soft_over_r, gamma_gas, **kw):
     if rc != DG_OK:
         raise DiskGPUError(rc, "dg_params_physical")
     return p, q.value
+
+
+def _records(rec):
+    """(n, 4) array of t, |C0|, |C2|, arg C2 -> ctypes Record array."""
+    rec = np.asarray(rec, dtype=np.float64).reshape(-1, 4)
+    arr = (Record * max(len(rec), 1))()
+    for k, (t, c0, c2, a2) in enumerate(rec):
+        arr[k].t, arr[k].c0, arr[k].c2, arr[k].arg2 = t, c0, c2, a2
+    return arr, len(rec)
+
+
+def fit_growth(rec, tmin=None, tmax=None):
+    """dg_fit_growth: FP64 least-squares gamma = d ln|C2|/dt and Omega_p = -1/2 d arg C2/dt
+    over tmin <= t <= tmax; returns (gamma, omega_p, n_points)."""
+    arr, n = _records(rec)
+    g, w, k = C.c_double(), C.c_double(), C.c_int()
+    rc = lib().dg_fit_growth(arr, n, np.nan if tmin is None else tmin, np.nan if tmax is None else tmax,
+                             C.byref(g), C.byref(w), C.byref(k))
+    if rc != DG_OK:
+        raise DiskGPUError(rc, lib().dg_last_error(None).decode())
+    return g.value, w.value, k.value
+
+
+def fit_phases(rec, t0=1.0, ratio_end=0.05, ratio_min=0.15):
+    """dg_fit_phases: ((gamma, Omega_p, n) of the linear phase, (|C2|/|C0|, Omega_p, n) of the
+    saturated phase)."""
+    arr, n = _records(rec)
+    out = np.zeros(6)
+    rc = lib().dg_fit_phases(arr, n, t0, ratio_end, ratio_min, _dp(out))
+    if rc != DG_OK:
+        raise DiskGPUError(rc, lib().dg_last_error(None).decode())
+    return (out[0], out[1], int(out[2])), (out[3], out[4], int(out[5]))
+
+
+def write_params(path, params_list):
+    """dg_params_write: the plain-text parameter file of a sweep (one disk per line)."""
+    arr = (Params * max(len(params_list), 1))(*[Params.from_buffer_copy(p) for p in params_list])
+    rc = lib().dg_params_write(os.fsencode(path), arr, len(params_list))
+    if rc != DG_OK:
+        raise DiskGPUError(rc, lib().dg_last_error(None).decode())
+
+
+def read_params(path, max_disks=1 << 16):
+    """dg_params_read: the disks of a parameter file as a list of Params."""
+    arr = (Params * max_disks)()
+    n = C.c_int()
+    rc = lib().dg_params_read(os.fsencode(path), arr, max_disks, C.byref(n))
+    if rc != DG_OK:
+        raise DiskGPUError(rc, lib().dg_last_error(None).decode())
+    return [Params.from_buffer_copy(arr[k]) for k in range(n.value)]
 
 
 class Disk:
@@ -309,9 +369,23 @@ class Disk:
         self._ck(lib().dg_time(self.h, C.byref(t), C.byref(n)))
         return t.value, n.value
 
-    def advance(self, tlim, cfl=0.3, dtout=0.25, max_rec=None):
+    def advance(self, tlim, cfl=0.3, dtout=0.25, max_rec=None, on_record=None):
         """Run the diskmain.cpp loop to tlim on the device; returns (records, t, steps)
-        with records an (n, 4) array of t, |C0|, |C2|, arg C2."""
+        with records an (n, 4) array of t, |C0|, |C2|, arg C2.  With on_record(t, c0, c2,
+        arg2) every record is also handed over as soon as the host drains it
+        (dg_advance_cb)."""
+        if on_record is not None:
+            got = []
+
+            def cb(r, _user):
+                rr = r.contents
+                got.append((rr.t, rr.c0, rr.c2, rr.arg2))
+                on_record(*got[-1])
+
+            fn = RECORD_FN(cb)
+            n, t, s = C.c_int(), C.c_double(), C.c_longlong()
+            self._ck(lib().dg_advance_cb(self.h, tlim, cfl, dtout, fn, None, C.byref(n), C.byref(t), C.byref(s)))
+            return np.array(got, dtype=np.float64).reshape(-1, 4), t.value, s.value
         t0, _ = self.time()
         if max_rec is None:
             max_rec = int(max(tlim - t0, 0) / dtout) + 8
@@ -351,6 +425,10 @@ class Disk:
     def run_steps(self, nsteps, cfl=0.3, sync=True):
         """nsteps device-resident steps with device-side dt (no host sync when sync=False)."""
         self._ck(lib().dg_run_steps(self.h, nsteps, cfl, 1 if sync else 0))
+
+    def capture_graph(self):
+        """Record the 64-step device-loop graph now, so no later call pays for it."""
+        self._ck(lib().dg_capture_graph(self.h))
 
     def step_host(self, Sig, vR, vp, cfl=0.3):
         """One reference-style step on host arrays (float64, C-contiguous), in place; returns dt."""

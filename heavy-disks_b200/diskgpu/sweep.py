@@ -103,3 +103,30 @@ def run_point(pt: SweepPoint, tlim: float, precision: str = "mixed", device: int
         g, w = float("nan"), float("nan")
     return {"index": pt.index, "gamma": g, "omega_p": w, "sat_ratio": saturation_ratio(rec[:, 1], rec[:, 2]),
             "Qmin_achieved": qach, "steps": int(steps), "t": t}
+
+
+def point_params(pt: SweepPoint, precision: str = "mixed", device: int = -1):
+    """The dg_params of a sweep disk: the physics dg_params_physical maps (Q_min,
+    M_d/M_*, softening/r, Gamma) to, on the point's grid, with its seed."""
+    from . import FP64, MIXED, params_physical
+
+    p, _ = params_physical(pt.Qmin, pt.mass_ratio, pt.soft_over_r, pt.gamma)
+    p.Nu = p.Nphi = pt.N
+    p.amp, p.phase0, p.device = pt.amp, pt.phase0, device
+    p.precision = {"fp64": FP64, "mixed": MIXED}[precision] if isinstance(precision, str) else precision
+    return p
+
+
+def write_sweep_file(path, points, precision: str = "mixed", device: int = -1):
+    """Describe a sweep outside Python: the plain-text parameter file (dg_params_write),
+    one disk per line with every dg_params field, readable by dg_params_read."""
+    from . import write_params
+
+    write_params(path, [point_params(pt, precision, device) for pt in points])
+
+
+def read_sweep_file(path):
+    """The disks of a parameter file (dg_params_read), ready for Batch or Disk(params=...)."""
+    from . import read_params
+
+    return read_params(path)

@@ -130,8 +130,49 @@ int dg_conserved(dg_handle *h, double *mass, double *angmom);
  * (up to max_rec); *n_rec, *t and *nsteps receive the counts and final time. */
 int dg_advance(dg_handle *h, double tlim, double cfl, double dtout, dg_record *rec, int max_rec,
                int *n_rec, double *t, long long *nsteps);
+/* Receiver of mode records for dg_advance_cb. */
+typedef void (*dg_record_fn)(const dg_record *rec, void *user);
+/* dg_advance that hands each record to fn(rec, user), in order, as soon as the host drains
+ * it from the device (after every chunk of at most 64 device steps) instead of collecting
+ * them: diskmain.cpp:93-98 prints and writes each record as it is made, and a long run
+ * keeps the records it made before a failure.  *n_rec (may be NULL) receives the count. */
+int dg_advance_cb(dg_handle *h, double tlim, double cfl, double dtout, dg_record_fn fn, void *user, int *n_rec,
+                  double *t, long long *nsteps);
 /* Simulation time and step count of the handle. */
 int dg_time(dg_handle *h, double *t, long long *nsteps);
+
+/* ---- Growth fit of the m = 2 mode (FP64, host only) ----
+ * The reference derived gamma and Omega_p off-line from diskfft_modes.dat
+ * (diskfft/README.md:26-29,37).  With the convention of Cm() (diskmain.cpp:72-84) a
+ * pattern rotating at Omega_p has arg C2 = -2 Omega_p t + const, so gamma = d ln|C2|/dt
+ * and Omega_p = -1/2 d arg C2/dt, arg C2 unwrapped over the records.
+ *
+ * Least squares over the records with tmin <= t <= tmax and |C2| > 0 (NaN for tmin or tmax
+ * means no bound); *npoints receives the count.  DG_ERR_INVALID with fewer than two. */
+int dg_fit_growth(const dg_record *rec, int n, double tmin, double tmax, double *gamma, double *omega_p,
+                  int *npoints);
+/* The two phases of a run through saturation, into out[6]:
+ *   out[0..2] gamma, Omega_p and the record count of the linear phase: from t0 (past the
+ *             seed's transient) until |C2|/|C0| first exceeds ratio_end (all records from
+ *             t0 / 2 on when that window holds fewer than four);
+ *   out[3..5] mean |C2|/|C0|, Omega_p and the record count of the saturated phase: from the
+ *             first to the last record with |C2|/|C0| >= ratio_min (NaN, NaN, 0 if fewer
+ *             than two).
+ * Typical thresholds: t0 = 1, ratio_end = 0.05, ratio_min = 0.15. */
+int dg_fit_phases(const dg_record *rec, int n, double t0, double ratio_end, double ratio_min, double *out);
+
+/* ---- Parameter file of a sweep (the reference takes positional argv only, diskmain.cpp:17-23) ----
+ * Plain text, one disk per line of blank-separated key=value pairs; '#' starts a comment.
+ * Keys are the dg_params field names (precision also takes fp64 | mixed, basic_state
+ * fft | elliptic).  A line may instead give a sweep point as Qmin, mass_ratio and
+ * soft_over_r (all three, with gamma_gas or its default 2): it is mapped through
+ * dg_params_physical first and any explicit field keys on the line apply after that.
+ * Unset fields take dg_params_default.  dg_params_write writes every field (doubles as
+ * %.17g), so reading the file back gives the same parameters bit for bit.  dg_params_read
+ * fills up to max entries and sets *n; a malformed line, an unknown key or more disks than
+ * max return DG_ERR_INVALID with the line number in dg_last_error(NULL). */
+int dg_params_write(const char *path, const dg_params *p, int n);
+int dg_params_read(const char *path, dg_params *p, int max, int *n);
 
 /* Snapshot / restart (new: the reference keeps its state only in the process).  The file
  * holds the parameters, t, the next record time, m_D, the step count, the full FP64
@@ -216,6 +257,12 @@ int dg_set_stream(dg_handle *h, void *stream);
  * With sync = 0 the call returns once the work is queued; a device-side error then shows
  * up at the next synchronising call. */
 int dg_run_steps(dg_handle *h, int nsteps, double cfl, int sync);
+/* Record the device loop's step graph now (64 steps; nothing runs).  dg_run_steps and
+ * dg_advance otherwise record it at their first full chunk, so a caller that times that
+ * call, or must not pay the recording at a later point, records it up front.  The graph
+ * holds the handle's stream and kernel choices: call after dg_set_stream and after the
+ * first state upload (which runs the autotuner). */
+int dg_capture_graph(dg_handle *h);
 /* One reference-style step on caller host buffers, in place: upload (Sig, vR, vp), then
  * timestep(cfl) -> potential -> forces -> step as diskmain.cpp:100-105, and download the
  * new state; *dt receives the dt used.  This is DiskHydro::step on host vectors. */
@@ -244,15 +291,18 @@ int dg_kernels_per_step(const dg_handle *h);
 int dg_tuning_info(const dg_handle *h, char *buf, int len);
 
 /* Allocation-free CFL time step.  No counterpart in the reference: it is the same
- * dt = cfl / max_ij (sR + sphi) as dg_timestep, for callers that may not allocate device
- * memory when they need it (while recording a CUDA graph, or when a pool or framework owns
- * all device memory).  Sig, vR, vp (Nu x Nphi, FP64, row-major) and dt (one double) are
- * DEVICE pointers owned by the caller; the grid is rebuilt from Nu, Nphi, Rin, Rout.  The
- * call allocates nothing: its scratch is a static per-device array of 8192 row maxima, so
+ * dt = cfl / max_ij (sR + sphi) as dg_timestep, for callers that must not allocate device
+ * memory when they need it (a pool or framework owns all device memory, or a fixed-budget
+ * loop must stay out of the allocator).  Sig, vR, vp (Nu x Nphi, FP64, row-major) and dt
+ * (one double) are DEVICE pointers owned by the caller; the grid is rebuilt from Nu, Nphi,
+ * Rin, Rout.  The call allocates nothing: its scratch is a static per-device array of 8192
+ * row maxima (64 KiB, held by every device that loads the library until exit), so
  * Nu > 8192 returns DG_ERR_UNSUPPORTED.  The first call on a device looks up that array's
- * address (make it before any stream capture).  Work is queued on `stream` (a
- * cudaStream_t as void*, NULL = default stream); the call does not synchronise.  All calls
- * share the scratch: calls that overlap on the GPU race. */
+ * address and keeps it for the process (make it before any stream capture; do not call
+ * again on a device after cudaDeviceReset).  Work is queued on `stream` (a cudaStream_t
+ * as void*, NULL = default stream); the call does not synchronise.  A non-finite state
+ * gives dt = NaN (the reference would skip the NaN).  All calls share the scratch: calls
+ * that overlap on the GPU race. */
 int dg_timestep_static(const double *Sig, const double *vR, const double *vp, int Nu, int Nphi, double Rin,
                        double Rout, double Kpoly, double gamma_gas, double cfl, double *dt, void *stream);
 
