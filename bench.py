@@ -8,17 +8,21 @@ zone-updates/s of the job, timed on the device as the max over ranks.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
                   [--size 1024] [--chunk 64] [--cold-steps 200] [--impl ours|reference]
 
-The K timed steps run as dg_run_steps calls of --chunk steps (each one launch of the
-captured step loop, the way dg_advance runs a disk), with L2 flushed before every call and
-CUDA events around it.  Then --cold-steps single steps, each after an L2 flush, give the
-cold per-step time and, with per-kernel events, the roofline of every kernel of the step.
-On one GPU the line also carries `fp64_same_disk` (the plain FP64 path on the same disk,
-timed the same way, and the mixed/FP64 ratio the metric names) and `batched_sweep` (256
-disks of the sweep law, grids 128^2..512^2, advanced together by dg_batch).
+After exactly W untimed warm-up steps, the K timed steps run as dg_run_steps calls of
+--chunk steps (each one launch of the captured step loop, the way dg_advance runs a disk;
+the graph is recorded before the warm-up, so no timed call pays for it), with L2 flushed
+before every call and CUDA events around it.  --repeats more timed regions of K steps give
+the spread.  Then --cold-steps single steps, each after an L2 flush, give the cold per-step
+time and, with per-kernel events, the roofline of every kernel of the step.  On one GPU the
+line also carries `fp64_same_disk` (the plain FP64 path on the same disk, timed over the
+same K steps, and the mixed/FP64 ratio the metric names), `cufft_gravity` (the same padded
+convolution through cuFFT, as a timing comparison only) and `batched_sweep` (256 disks of
+the sweep law, grids 128^2..512^2, advanced together by dg_batch).
 
 --impl reference times the reference's own CPU implementation (diskfft/src hydro.hpp +
-kalnajs.hpp compiled unmodified against the FFTW-API shim, oracle/_ref/refbench) on the
-host cores for the same workload; under torchrun only rank 0 runs it.
+kalnajs.hpp compiled unmodified against the FFTW-API shim, with the reference Makefile's
+-O3 and FP contraction: oracle/_ref/refbench_fast_v4, or _v3 on hosts without AVX-512) on
+the host cores for the same workload; under torchrun only rank 0 runs it.
 """
 from __future__ import annotations
 
@@ -36,7 +40,23 @@ sys.path.insert(0, os.path.join(ROOT, "heavy-disks_b200"))
 
 METRIC = "zone-updates/s/GPU (hydro+FFT gravity), mixed vs FP64 plain at matched γ,Ω_p"
 UNIT = "zone-updates/s"
-REFBENCH = os.path.join(ROOT, "oracle", "_ref", "refbench")
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def refbench_path():
+    """The timing build of the reference for this host: x86-64-v4 where the CPU has
+    AVX-512 (the reference Makefile's -march=native on such hosts), else x86-64-v3."""
+    avx512 = False
+    try:
+        with open("/proc/cpuinfo") as f:
+            avx512 = any(l.startswith("flags") and " avx512f" in l for l in f)
+    except OSError:
+        pass
+    for name in (("refbench_fast_v4",) if avx512 else ()) + ("refbench_fast_v3", "refbench"):
+        p = os.path.join(REF_DIR, name)
+        if os.path.exists(p):
+            return p
+    return None
 
 
 def parse():
@@ -52,8 +72,10 @@ def parse():
     ap.add_argument("--chunk", type=int, default=64, help="steps per timed iteration (one graph launch)")
     ap.add_argument("--cold-steps", type=int, default=200,
                     help="single steps with a flushed L2, timed and profiled per kernel")
-    ap.add_argument("--fp64-steps", type=int, default=1024,
-                    help="steps of the plain FP64 path on the same disk (0: skip the comparison)")
+    ap.add_argument("--fp64-steps", type=int, default=None,
+                    help="steps of the plain FP64 path on the same disk (default: --steps; 0: skip it)")
+    ap.add_argument("--repeats", type=int, default=5, help="extra timed regions of K steps for the spread")
+    ap.add_argument("--cufft", type=int, default=1, help="time the cuFFT form of the gravity (0: skip)")
     ap.add_argument("--batch-disks", type=int, default=256,
                     help="disks of the batched sweep measurement (0: skip it)")
     ap.add_argument("--batch-tlim", type=float, default=0.1, help="time the batched sweep advances")
@@ -74,7 +96,7 @@ def workload(a):
 # CPU reference (host cores)
 
 def run_refbench(size, eps, threads, warm, steps):
-    out = subprocess.run([REFBENCH, str(size), str(size), repr(eps), str(threads), str(warm), str(steps)],
+    out = subprocess.run([refbench_path(), str(size), str(size), repr(eps), str(threads), str(warm), str(steps)],
                          capture_output=True, text=True, check=True).stdout
     return json.loads(out.strip().splitlines()[-1])
 
@@ -82,7 +104,7 @@ def run_refbench(size, eps, threads, warm, steps):
 def cpu_sample(size, eps, seconds=10.0):
     """Bounded sample of the reference build: estimate the step time, then time ~`seconds`."""
     threads = os.cpu_count() or 1
-    if not os.path.exists(REFBENCH):
+    if refbench_path() is None:
         return None
     probe = run_refbench(size, eps, threads, 1, 2)
     per = probe["seconds"] / 2
@@ -91,13 +113,14 @@ def cpu_sample(size, eps, seconds=10.0):
     return {"value": r["zone_updates_per_s"], "unit": UNIT, "cores": threads, "kind": "reference",
             "sample": f"{steps} steps of the {size}x{size} disk (eps {eps}) by the reference's DiskHydro + "
                       f"KalnajsSolver compiled unmodified with the project FFTW-API shim (not FFTW), "
-                      f"{threads} OpenMP threads, wall clock"}
+                      f"-O3 with FP contraction ({os.path.basename(refbench_path())}), {threads} OpenMP "
+                      f"threads, wall clock"}
 
 
 def reference_arm(a, rank):
     if rank != 0:
         return
-    if not os.path.exists(REFBENCH):
+    if refbench_path() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/refbench not built"}))
         return
     threads = os.cpu_count() or 1
@@ -109,7 +132,8 @@ def reference_arm(a, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload(a),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": f"{a.steps} timed steps after {max(a.warmup, 1)} warm-up, reference "
-                                   "sources compiled unmodified with the project FFTW-API shim"},
+                                   "sources compiled unmodified with the project FFTW-API shim, -O3 with FP "
+                                   f"contraction ({os.path.basename(refbench_path())})"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -251,17 +275,29 @@ def gravity_parts(precision, Nu, Nphi):
             ("grav_phi_inv", g4name, "tensor", g4, "flop")]
 
 
-def timed_chunks(disk, stream, flush, steps, chunk):
-    """Device milliseconds of `steps` steps of `disk` run as dg_run_steps calls of `chunk`
-    steps (after 3 untimed calls), with L2 flushed before every call and CUDA events
-    around each."""
-    import torch
+def chunk_sizes(steps, chunk):
     chunk = max(1, min(chunk, steps))
-    sizes = [chunk] * (steps // chunk) + ([steps % chunk] if steps % chunk else [])
+    return [chunk] * (steps // chunk) + ([steps % chunk] if steps % chunk else [])
+
+
+def warm_up(disk, stream, flush, warmup, chunk):
+    """Exactly `warmup` untimed steps as dg_run_steps calls of up to `chunk` steps, after
+    recording the step graph (which runs nothing)."""
+    import torch
+    disk.capture_graph()
     with torch.cuda.stream(stream):
-        for _ in range(3):
+        for n in (chunk_sizes(warmup, chunk) if warmup > 0 else []):
             flush.zero_()
-            disk.run_steps(chunk, 0.3, sync=False)
+            disk.run_steps(n, 0.3, sync=False)
+        torch.cuda.synchronize()
+
+
+def timed_region(disk, stream, flush, steps, chunk):
+    """Device milliseconds of `steps` steps run as dg_run_steps calls of `chunk` steps, L2
+    flushed before every call (outside the events), CUDA events around each call."""
+    import torch
+    sizes = chunk_sizes(steps, chunk)
+    with torch.cuda.stream(stream):
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in sizes]
         for k, n in enumerate(sizes):
             flush.zero_()
@@ -269,21 +305,99 @@ def timed_chunks(disk, stream, flush, steps, chunk):
             disk.run_steps(n, 0.3, sync=False)
             ev[k][1].record(stream)
         torch.cuda.synchronize()
-    disk.run_steps(0, 0.3, sync=True)
     return sum(b.elapsed_time(e) for b, e in ev)
 
 
-def fp64_same_disk(a, device, stream, flush, phase0):
-    """The plain FP64 path (the reference's arithmetic) on the same disk, timed the same way."""
+def spread(ms_list, steps):
+    per = sorted(m / steps for m in ms_list)
+    return {"regions": len(per), "median_ms_per_step": statistics.median(per), "min_ms_per_step": per[0],
+            "max_ms_per_step": per[-1]}
+
+
+def fp64_same_disk(a, device, stream, flush, phase0, steps, chunk):
+    """The plain FP64 path (the reference's arithmetic) on the same disk, with the same
+    warm-up, the same K timed steps in the same chunks, and the same repeats."""
     import diskgpu as D
     N = a.size
     with D.Disk(N, N, eps=a.eps, amp=1e-3, precision="fp64", phase0=phase0, device=device) as d:
         d.init_standard()
         d.set_stream(stream.cuda_stream)
-        ms = timed_chunks(d, stream, flush, a.fp64_steps, a.chunk)
-    return {"value": N * N * a.fp64_steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / a.fp64_steps,
-            "steps": a.fp64_steps, "how": "same disk and timing as the headline, precision fp64 (k_hydro64 + "
-                                          "three shared-memory FFT passes)"}
+        warm_up(d, stream, flush, max(a.warmup, 3), chunk)
+        ms = timed_region(d, stream, flush, steps, chunk)
+        reps = [timed_region(d, stream, flush, steps, chunk) for _ in range(a.repeats)]
+        d.run_steps(0, 0.3, sync=True)
+    return {"value": N * N * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+            "repeats": spread(reps, steps) if reps else None,
+            "how": "same disk, warm-up, K steps, chunks and L2 flushes as the headline, precision fp64 "
+                   "(k_hydro64 + three shared-memory FFT passes)"}
+
+
+def khat_table(Nu, Nphi, eps):
+    """The Green's-function spectrum of kalnajs.hpp:105-116 (r2c of the softened kernel at
+    wrapped radial offsets), real and even, FP64: the multiplier of the cuFFT comparison."""
+    import numpy as np
+    M = 2 * Nu
+    du, dphi = np.log(4.0) / Nu, 2 * np.pi / Nphi
+    p = np.arange(M)
+    ioff = np.where(p <= M // 2, p, p - M)
+    K = 1.0 / np.sqrt(2.0 * np.cosh(ioff * du)[:, None] - 2.0 * np.cos(np.arange(Nphi) * dphi)[None, :] + eps)
+    return np.fft.rfft2(K)
+
+
+def cufft_gravity(a, device, flush, disk64_potential):
+    """Timing comparison only (the product never calls cuFFT): the same zero-padded
+    2 Nu x Nphi convolution as kalnajs.hpp:48-63 through cuFFT (torch.fft: D2Z / Z2D in
+    FP64, R2C / C2R in FP32), with the khat multiply, padding and scaling as torch
+    elementwise kernels, recorded in a CUDA graph and replayed after an L2 flush."""
+    import numpy as np
+    import torch
+    N = a.size
+    Nu = Nphi = N
+    M = 2 * Nu
+    du, dphi = np.log(4.0) / Nu, 2 * np.pi / Nphi
+    R = np.exp(np.log(0.25) + (np.arange(Nu) + 0.5) * du)
+    kh = khat_table(Nu, Nphi, a.eps)
+    rng = np.random.default_rng(5)
+    S0 = 0.372 * np.exp(-(R - 0.45) ** 2 / 0.05)
+    Sig = S0[:, None] * (1 + 1e-3 * np.cos(2 * (np.arange(Nphi) + 0.5) * dphi))[None, :] + 1e-4 * rng.random((Nu, Nphi))
+    ref = disk64_potential(Sig)
+    out = {}
+    for dt, name in ((torch.float64, "fp64"), (torch.float32, "fp32")):
+        ct = torch.complex128 if dt == torch.float64 else torch.complex64
+        khd = torch.from_numpy(kh).to(device=f"cuda:{device}", dtype=ct)
+        r32 = torch.from_numpy(R ** 1.5).to(device=f"cuda:{device}", dtype=dt)[:, None]
+        sc = torch.from_numpy(-du * dphi / np.sqrt(R)).to(device=f"cuda:{device}", dtype=dt)[:, None]
+        sig = torch.from_numpy(Sig).to(device=f"cuda:{device}", dtype=dt)
+        pad = torch.zeros((M, Nphi), dtype=dt, device=f"cuda:{device}")
+        phi = torch.empty((Nu, Nphi), dtype=dt, device=f"cuda:{device}")
+
+        def conv():
+            pad[:Nu].copy_(sig * r32)
+            v = torch.fft.irfft2(torch.fft.rfft2(pad) * khd, s=(M, Nphi))
+            phi.copy_(v[:Nu] * sc)
+
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(3):
+                conv()
+        torch.cuda.current_stream().wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            conv()
+        reps = 50
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for b, e in ev:
+            flush.zero_()
+            b.record()
+            g.replay()
+            e.record()
+        torch.cuda.synchronize()
+        ms = sum(b.elapsed_time(e) for b, e in ev) / reps
+        err = float(np.max(np.abs(phi.double().cpu().numpy() - ref)) / np.max(np.abs(ref)))
+        out[name] = {"ms_per_convolution": ms, "rel_err_vs_fp64_path": err}
+        del g
+    return out
 
 
 def batched_sweep(a, device):
@@ -353,35 +467,26 @@ def main():
     kps = disk.kernels_per_step()
 
     # timed iterations: one dg_run_steps call of `chunk` steps each (a CUDA graph of the
-    # device-resident step loop, as dg_advance runs it), L2 flushed before every iteration
+    # device-resident step loop, as dg_advance runs it), L2 flushed before every iteration;
+    # exactly W warm-up steps before them, the graph recorded first
     chunk = max(1, min(a.chunk, a.steps))
-    sizes = [chunk] * (a.steps // chunk) + ([a.steps % chunk] if a.steps % chunk else [])
-    warm_iters = max(3, -(-a.warmup // chunk))
-
+    warm = max(a.warmup, 3)
     clk = ClockSampler(physical_gpu_index(local)).__enter__()
-    with torch.cuda.stream(stream):
-        for _ in range(warm_iters):
-            flush.zero_()
-            disk.run_steps(chunk, 0.3, sync=False)
-        torch.cuda.synchronize()
-
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in sizes]
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        t_wall0 = time.time()
-        for k, n in enumerate(sizes):
-            flush.zero_()
-            ev[k][0].record(stream)
-            disk.run_steps(n, 0.3, sync=False)
-            ev[k][1].record(stream)
-        torch.cuda.synchronize()
-        clk.window = (t_wall0, time.time())
-        clk.__exit__(None, None, None)
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        ms = sum(s.elapsed_time(e) for s, e in ev)
+    warm_up(disk, stream, flush, warm, chunk)
+    t_wait = time.time()
+    while clk.proc and not clk.lines and time.time() - t_wait < 3.0:  # the sampler is running
+        time.sleep(0.02)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_wall0 = time.time()
+    ms = timed_region(disk, stream, flush, a.steps, chunk)
+    clk.window = (t_wall0, time.time())
+    clk.__exit__(None, None, None)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    reps = [timed_region(disk, stream, flush, a.steps, chunk) for _ in range(a.repeats)]
     t_dev = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
@@ -477,11 +582,23 @@ def main():
             e2e["value"] = world * zones * a.e2e_steps / float(t_e.item())
 
     # ---- the plain FP64 path on the same disk, and a batched sweep (one rank) ----
-    fp64 = batch = None
+    fp64 = batch = cufft = None
     if world == 1 and a.precision == "mixed":
-        if a.fp64_steps > 0:
-            fp64 = fp64_same_disk(a, local, stream, flush, phase0)
+        f64_steps = a.steps if a.fp64_steps is None else a.fp64_steps
+        if f64_steps > 0:
+            fp64 = fp64_same_disk(a, local, stream, flush, phase0, f64_steps, chunk)
             fp64["mixed_over_fp64"] = value / fp64["value"]
+            if reps and fp64.get("repeats"):
+                fp64["mixed_over_fp64_median_of_repeats"] = (fp64["repeats"]["median_ms_per_step"] /
+                                                             spread(reps, a.steps)["median_ms_per_step"])
+        if a.cufft:
+            with D.Disk(N, N, eps=a.eps, precision="fp64", device=local) as d64:
+                cufft = cufft_gravity(a, local, flush, d64.potential)
+            grav_ms = sum(prof[k][0] / prof[k][1] for k in ("grav_phi_fwd", "grav_u", "grav_phi_inv") if prof[k][1])
+            cufft["tcgen05_gravity_ms"] = grav_ms
+            cufft["note"] = ("timing comparison only: cuFFT through torch.fft on the same padded "
+                             f"{2 * N}x{N} convolution, graph-replayed after an L2 flush; tcgen05_gravity_ms = the "
+                             "mixed step's three gravity kernels, each timed alone after an L2 flush")
         if a.batch_disks > 0:
             batch = batched_sweep(a, local)
 
@@ -503,13 +620,14 @@ def main():
                     "kernels_per_step": kps, "autotuner": disk.tuning()})
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-            "warmup": warm_iters * chunk, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
+            "warmup": warm, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if a.precision == "fp64" else "f32 state + f64 basic state, split-bf16 DFT",
             "data": "synthetic (standard heavy disk, seeded m=2 phase)", "config": cfg,
             "roofline": roof, "roofline_all": roof_all, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": kps * a.steps, "clocks": clk.summary(),
-            "fp64_same_disk": fp64, "batched_sweep": batch,
+            "repeats": spread(reps, a.steps) if reps else None,
+            "fp64_same_disk": fp64, "cufft_gravity": cufft, "batched_sweep": batch,
         }
         print(json.dumps(line))
     disk.close()

@@ -102,7 +102,16 @@ struct MixedState {
   float2 *twp = nullptr; // W_M^{p2 i1} with padded rows, [64][kUcTwLd]
   CUtensorMap mXin[2], mTb[2], mYk[2], mUb[2], mRB[2], mRA[2], mRGA[2], mRGB[2], mZmn[2];
   bool tables_ready = false;
+  // Failure-detection test: DISKGPU_TEST_ROWTILE_STALL=<row tile> at handle creation makes
+  // the first self-gravity step enqueued outside a graph capture raise that tile row's
+  // counter once more after its hydro has finished, so the next phi transform's bounded
+  // wait on it runs out (~1 s) and the step reports DG_ERR_TIMEOUT.  Off (-1) otherwise.
+  int test_stall = -1;
 };
+
+// One extra count on a row-tile counter (the failure-detection test above): no hydro CTA
+// will count it down.  Launched in plain stream order, so the hydro before it has finished.
+__global__ void k_rowtile_stall(int *cnt) { atomicAdd(cnt, 1); }
 
 // ---------------------------------------------------------------------------------
 // TMA descriptors
@@ -722,6 +731,13 @@ int dg_handle::mixed_init() {
       if (!okh) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed (hydro tiles)");
     }
   }
+  {
+    const char *ts = getenv("DISKGPU_TEST_ROWTILE_STALL");
+    if (ts && *ts) {
+      const int k = atoi(ts);
+      if (k >= 0 && k < (Nu + kTileI - 1) / kTileI) X.test_stall = k;
+    }
+  }
   X.tables_ready = true;
   return DG_OK;
 }
@@ -1257,6 +1273,12 @@ int dg_handle::mixed_gravity() {
   return DG_OK;
 }
 
+// whether the last enqueued hydro counted down the row-tile counters (prev_rs)
+int dg_handle::loop_flags() const { return (mx && mx->prev_rs) ? 1 : 0; }
+void dg_handle::set_loop_flags(int f) {
+  if (mx) mx->prev_rs = (f & 1) != 0;
+}
+
 // the tile forms end with k_step_finalize
 int dg_handle::mixed_hydro_kernels() const {
   return (mx && mx->hydro_kind != MixedState::kHydroWarp) ? 2 : 1;
@@ -1292,6 +1314,15 @@ int dg_handle::mixed_enqueue_step() {
   X.prev_rs = rs;
   XK(prof_end(DG_PROF_HYDRO));  // the hydro kernel alone; its finalisation follows
   XK(launch_finalize(X, ctl, st));
+  if (rs && X.test_stall >= 0) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    XK(cudaStreamIsCapturing(st, &cs));
+    if (cs == cudaStreamCaptureStatusNone) {
+      k_rowtile_stall<<<1, 1, 0, st>>>(X.rowpend + X.test_stall);
+      XK(cudaGetLastError());
+      X.test_stall = -1;
+    }
+  }
   cur = o;
   return DG_OK;
 }

@@ -1,9 +1,9 @@
 // Allocation-free variant of the CFL time step (dg_timestep_static, include/diskgpu.h).
 //
-// Some callers cannot allocate device memory at the moment they need a time step: code
-// that is recording a CUDA graph (an allocation would break or be illegal inside the
-// capture), hosts whose device memory is owned by a pool or framework that forbids any
-// other allocation after start-up, and fixed-budget real-time loops.  This entry point
+// Some callers cannot allocate device memory at the moment they need a time step: hosts
+// whose device memory is owned by a pool or framework that forbids any other allocation
+// after start-up, and fixed-budget loops that must not call into the allocator (a
+// cudaMalloc can synchronise the device and its cost is unbounded).  This entry point
 // computes dt = cfl / max_ij (sR + sphi) (the reference's DiskHydro::timestep) from
 // caller-owned device arrays into a caller-owned device double, using no memory of its
 // own except the file-scope scratch array below.
@@ -11,7 +11,10 @@
 // The scratch holds one per-row maximum, so the largest grid is kMaxRows radial rows.
 // It lives in every device that loads this library until the process exits.  Its device
 // address is looked up once per device (cudaGetSymbolAddress) on the first call made with
-// that device current; make that first call before any stream capture.  All calls share
+// that device current; make that first call before any stream capture.  The looked-up
+// address is kept for the life of the process: after cudaDeviceReset on a device, this
+// entry point must not be called on that device again.  A non-finite value in the state
+// makes dt NaN (the reference's std::max would skip it).  All calls share
 // the one array and it keeps the last call's contents: calls that overlap on the GPU
 // (different streams, no ordering between them) race on it.  Every row slot a call reads
 // is written by the same call first, so nothing needs clearing between calls.
@@ -102,6 +105,8 @@ extern "C" int dg_timestep_static(const double *Sig, const double *vR, const dou
   const double umin = std::log(Rin), umax = std::log(Rout);
   const double du = (umax - umin) / Nu, dphi = 2.0 * M_PI / Nphi;
   cudaStream_t st = (cudaStream_t)stream;
+  // an error left by earlier work is not this call's: report it without launching
+  if (cudaPeekAtLastError() != cudaSuccess) return DG_ERR_CUDA;
   k_cfl_rows<<<Nu, 256, 0, st>>>(Sig, vR, vp, Nphi, umin, du, dphi, Kpoly, gamma_gas, scratch);
   if (cudaGetLastError() != cudaSuccess) return DG_ERR_CUDA;
   k_cfl_rows_to_dt<<<1, 256, 0, st>>>(scratch, Nu, cfl, dt);

@@ -7,7 +7,7 @@ fixed LKA98 value, then Newton; eigensolve.py:156-211) and the seeded route (a c
 calls and wall time.  Needs the reference tree (lka98 is imported from it) and
 numpy/scipy; no GPU:
 
-    python tests/golden/make_lka98_seed.py [--ref /root/reference] [--sizes 100 300]
+    python tests/golden/make_lka98_seed.py [--ref REFERENCE_ROOT (default: $HEAVY_DISKS_REFERENCE)] [--sizes 100 300]
 """
 import argparse
 import json
@@ -37,7 +37,7 @@ def surrogate_seed():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("HEAVY_DISKS_REFERENCE", "/root/reference"))
     ap.add_argument("--sizes", type=int, nargs="+", default=[100, 300])
     a = ap.parse_args()
     sys.path.insert(0, a.ref)

@@ -26,9 +26,13 @@ def _field(Nu, Nphi, seed=0):
     return S0[:, None] * (1 + pert) + 1e-3 * rng.random((Nu, Nphi))
 
 
-@pytest.mark.parametrize("Nu,Nphi", [(128, 128), (256, 256), (128, 384), (512, 256), (1024, 256), (1024, 1024)])
+@pytest.mark.parametrize("Nu,Nphi", [(128, 128), (256, 256), (128, 384), (512, 256), (1024, 256), (1024, 1024),
+                                     (2048, 128), (4096, 128), (128, 2048), (128, 4096)])
 def test_tensor_core_potential_vs_fp64(Nu, Nphi):
-    """The 4-GEMM split-BF16 DFT convolution against the FP64 FFT potential (<= 2e-4 rel)."""
+    """The split-BF16 DFT convolution against the FP64 FFT potential (<= 2e-4 rel).  The
+    grids reach every form: dense u and phi products (128..512), the fused transforms
+    (1024^2), the four-pass factored u convolution with A = 64 and 128 (Nu = 2048, 4096)
+    and the dense phi products at K = 2048 and 4096."""
     Sig = _field(Nu, Nphi)
     ref = O.Kalnajs(Nu, Nphi, eps=0.01).potential(Sig)
     with D.Disk(Nu, Nphi, eps=0.01, precision="mixed") as d:
@@ -114,6 +118,27 @@ def test_growth_and_saturation_match_fp64_1024():
     assert abs(gmx - g64) <= 5e-3 * abs(g64), (gmx, g64)
     assert abs(wmx - w64) <= 5e-3 * abs(w64), (wmx, w64)
     assert abs(rmx - r64) <= 0.02 * r64, (rmx, r64)
+
+
+def test_4096_disk_conservation_and_diagnostics():
+    """The large single disk (4096^2, gravity on the 8192 x 4096 padded grid, mixed
+    precision) for 300 device steps with the per-step m = 0..8 diagnostic on: one ring row
+    per step, C_0 = mass / m_D stays 1, and the FP64 global sums drift by no more than
+    round-off (mass) and the scheme's small truncation error (angular momentum; the
+    reference's transport is not exactly angular-momentum conserving)."""
+    with D.Disk(4096, 4096, eps=0.005, amp=1e-3, precision="mixed") as d:
+        d.init_standard()
+        d.set_diagnostics(8, 1024)
+        m0, L0 = d.conserved()
+        d.run_steps(300, 0.3)
+        m1, L1 = d.conserved()
+        t, C = d.diagnostics()
+    assert len(t) == 300 and C.shape == (300, 9)
+    assert np.all(np.diff(t) > 0)
+    assert np.max(np.abs(C[:, 0] - 1.0)) < 1e-9
+    assert abs(C[-1, 2]) > 0.5e-3  # the m = 2 seed is carried
+    assert abs(m1 - m0) <= 1e-11 * m0, (m1 - m0) / m0
+    assert abs(L1 - L0) <= 1e-8 * abs(L0), (L1 - L0) / L0
 
 
 def test_mixed_requires_multiple_of_128():
@@ -213,3 +238,72 @@ def test_row_tile_handover_is_bit_identical(monkeypatch):
     assert ta == tb
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
+
+
+def test_rowtile_wait_timeout_is_reported_and_handle_recovers(monkeypatch):
+    """Failure detection without a GPU fault: DISKGPU_TEST_ROWTILE_STALL=<tile row> makes one
+    row-tile counter stay above zero after the first step's hydro finished, so the second
+    step's phi transform gives up its bounded wait (~1 s of SM clock; its own TMA copies are
+    valid and are drained before it exits) and raises the timeout status.  The host returns
+    DG_ERR_TIMEOUT; a new state clears the status and the counters, and the same handle then
+    steps bit-identically to a fresh one."""
+    import time
+    monkeypatch.setenv("DISKGPU_TUNE", "0")
+    monkeypatch.delenv("DISKGPU_HYDRO32", raising=False)
+    monkeypatch.delenv("DISKGPU_ROWSYNC", raising=False)
+    monkeypatch.setenv("DISKGPU_TEST_ROWTILE_STALL", "20")
+    with D.Disk(1024, 1024, eps=0.005, amp=1e-3, precision="mixed") as d:
+        d.init_standard()
+        S, vR, vp = d.get_state()
+        t0 = time.time()
+        with pytest.raises(D.DiskGPUError) as e:
+            d.run_steps(4, 0.3)
+        assert e.value.code == -6, e.value
+        assert time.time() - t0 < 30
+        d.set_state(S, vR, vp)
+        d.run_steps(4, 0.3)
+        got = d.get_state()
+    monkeypatch.delenv("DISKGPU_TEST_ROWTILE_STALL")
+    with D.Disk(1024, 1024, eps=0.005, amp=1e-3, precision="mixed") as f:
+        f.set_state(S, vR, vp)
+        f.run_steps(4, 0.3)
+        want = f.get_state()
+    for x, y in zip(got, want):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_capture_graph_up_front_changes_nothing(monkeypatch):
+    """dg_capture_graph records the 64-step graph without running it: stepping afterwards
+    (single steps, then graph launches, with the row-tile hand-over at 1024^2) gives the
+    state bit for bit that the same steps give with the graph recorded on first use."""
+    monkeypatch.delenv("DISKGPU_ROWSYNC", raising=False)
+    out = []
+    for pre in (True, False):
+        with D.Disk(1024, 1024, eps=0.005, amp=1e-2, precision="mixed") as d:
+            d.init_standard()
+            if pre:
+                d.capture_graph()
+            d.run_steps(6, 0.3)
+            d.run_steps(128, 0.3)
+            d.run_steps(3, 0.3)
+            out.append((d.get_state(), d.time()))
+    (a, ta), (b, tb) = out
+    assert ta == tb
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_advance_with_record_callback_matches_advance(prec):
+    """dg_advance_cb hands over the same records, in order, as dg_advance collects."""
+    runs = []
+    for cb in (False, True):
+        seen = []
+        with D.Disk(128, 128, eps=0.01, amp=1e-3, precision=prec) as d:
+            d.init_standard()
+            rec, t, n = d.advance(3.0, on_record=(lambda *r: seen.append(r)) if cb else None)
+        runs.append((rec, t, n))
+        if cb:
+            np.testing.assert_array_equal(np.array(seen), rec)
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    assert runs[0][1:] == runs[1][1:]

@@ -1,7 +1,10 @@
-"""dg_timestep_static: the CFL time step for callers that may not allocate device memory
-(for example while recording a CUDA graph, or when a memory pool owns the device).  It
-must agree with dg_timestep on the same state, on two calls in a row, with nothing of its
-own allocated (its scratch is a static per-device array).  Collected last on purpose."""
+"""dg_timestep_static: the CFL time step for callers that must not allocate device memory
+(a memory pool or framework owns the device, or a fixed-budget loop must stay out of the
+allocator).  It must agree with dg_timestep on the same state, on two calls in a row, with
+nothing of its own allocated (its scratch is a static per-device array): the device's free
+memory is the same before and after those calls.  The first call on a device may load the
+library's device code and looks up the scratch address, so the free-memory check starts
+after it.  Collected last on purpose."""
 import ctypes as C
 
 import numpy as np
@@ -26,12 +29,18 @@ def test_static_timestep_matches_dg_timestep_twice():
         d.init_standard()
         dt_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
         stream = torch.cuda.current_stream().cuda_stream
+        S, vR, vp = d.get_state()
+        warm = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (S, vR, vp)]
+        _call_static(warm, d.p, 0.3, dt_dev, stream)  # set-up call (scratch address lookup)
+        torch.cuda.synchronize()
         for call in range(2):
             S, vR, vp = d.get_state()
             dev = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (S, vR, vp)]
             torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info()[0]
             _call_static(dev, d.p, 0.3, dt_dev, stream)
             torch.cuda.synchronize()
+            assert torch.cuda.mem_get_info()[0] == free0, "the call changed the device's free memory"
             got = float(dt_dev.item())
             want = d.timestep(0.3)
             assert got == pytest.approx(want, rel=1e-12), (call, got, want)
