@@ -1,13 +1,19 @@
 // Batched sweeps: many independent disks (heterogeneous grids and parameters) advanced
-// together by one CUDA graph per launch.  The graph forks one branch per disk from a
-// root stream; each branch holds that disk's steps (gravity + hydro kernels) on the disk's
-// own stream, so the disks' kernels overlap on the GPU, and joins back.  Every disk keeps
-// its own device-resident dt, time and record ring (dg::Ctl); a disk that reaches tlim
-// turns the rest of its branch into pass-through launches.  Disks with a smaller dt get
+// together by one CUDA graph per launch.  Mixed-precision disks that share a grid, a
+// Gamma class (Gamma = 2 or not), a hydro kernel form and product pipeline depths form a
+// group: one launch per kernel advances the whole group (mixed.cu, disk groups), the disk
+// in blockIdx.z.  Every other disk is a branch of its own, holding its single-disk steps.
+// The graph forks one branch per group or lone disk from a root stream, each on its own
+// stream, so the branches overlap on the GPU, and joins back.  Every disk keeps its own
+// device-resident dt, time and record ring (dg::Ctl); a disk that reaches tlim turns the
+// rest of its launches into pass-throughs.  Branches whose disks have a smaller dt get
 // proportionally more steps per launch so that the branches finish together.
+// DISKGPU_BATCH_GROUPS=0 in the environment turns grouping off (every disk its own branch).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -19,6 +25,7 @@ struct dg_batch {
   cudaStream_t root = nullptr;
   cudaGraphExec_t exec = nullptr;
   std::vector<cudaEvent_t> events;
+  std::vector<MixedGroup *> groups;  // the groups the captured graph launches
   int dev = -1;
   std::string err;
   int fail(int code, const char *what, const char *why) {
@@ -28,6 +35,8 @@ struct dg_batch {
   void release_graph() {
     if (exec) cudaGraphExecDestroy(exec);
     exec = nullptr;
+    for (MixedGroup *g : groups) mixed_group_destroy(g);
+    groups.clear();
   }
 };
 
@@ -144,22 +153,58 @@ int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int ste
       s = std::max(2, s + (s & 1));
       b->steps_per_launch[k] = s;
     }
-    // capture: root -> fork to every disk stream -> K_k steps each -> join
+    // branches: groups of same-grid mixed disks, and lone disks
+    std::vector<std::vector<int>> branches;
+    {
+      const char *ge = getenv("DISKGPU_BATCH_GROUPS");
+      const bool grouping = !(ge && strcmp(ge, "0") == 0);
+      std::map<std::string, std::vector<int>> by_key;
+      for (int k = 0; k < n; ++k) {
+        const std::string key = grouping ? mixed_group_key(b->disks[k]) : std::string();
+        if (key.empty()) branches.emplace_back(1, k);
+        else by_key[key].push_back(k);
+      }
+      for (auto &kv : by_key) {
+        if (kv.second.size() == 1) {
+          branches.emplace_back(1, kv.second[0]);
+          continue;
+        }
+        std::vector<dg_handle *> members;
+        for (int k : kv.second) members.push_back(b->disks[k]);
+        std::string why;
+        MixedGroup *grp = mixed_group_create(members, &why);
+        if (!grp) return b->fail(DG_ERR_CUDA, "dg_batch_advance", why.c_str());
+        b->groups.push_back(grp);
+        branches.emplace_back(std::move(kv.second));
+      }
+    }
+    // capture: root -> fork to every branch's stream -> its steps -> join
     for (dg_handle *h : b->disks) {
       int rc0 = h->prof_collect();
       if (rc0) return b->fail(rc0, "dg_batch_advance", h->err.c_str());
       h->prof_on = false;  // no event timing inside the batch graph
     }
+    b->events.resize(n + 1);
     cudaGraph_t g = nullptr;
     BK(cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal));
     cudaEventRecord(b->events[n], b->root);
     int rc = DG_OK;
-    for (int k = 0; k < n && !rc; ++k) {
-      dg_handle *h = b->disks[k];
+    size_t gi = 0;
+    for (size_t q = 0; q < branches.size() && !rc; ++q) {
+      const std::vector<int> &br = branches[q];
+      dg_handle *h = b->disks[br[0]];
+      int steps = 0;
+      for (int k : br) steps = std::max(steps, b->steps_per_launch[k]);
       cudaStreamWaitEvent(h->st, b->events[n], 0);
-      for (int s = 0; s < b->steps_per_launch[k] && !rc; ++s) rc = h->enqueue_step();
-      cudaEventRecord(b->events[k], h->st);
-      cudaStreamWaitEvent(b->root, b->events[k], 0);
+      if (br.size() > 1) {
+        MixedGroup *grp = b->groups[gi++];
+        for (int s = 0; s < steps && !rc; ++s) rc = mixed_group_enqueue_step(grp, h->st);
+        if (rc) rc = b->fail(rc, "dg_batch_advance", h->err.c_str());
+      } else {
+        for (int s = 0; s < steps && !rc; ++s) rc = h->enqueue_step();
+      }
+      cudaEventRecord(b->events[q], h->st);
+      cudaStreamWaitEvent(b->root, b->events[q], 0);
     }
     cudaError_t e = cudaStreamEndCapture(b->root, &g);
     for (dg_handle *h : b->disks) h->cur = 0;  // capture flipped the buffers an even number of times

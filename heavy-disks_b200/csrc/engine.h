@@ -8,6 +8,14 @@
 #include "kernels.h"
 
 struct MixedState;  // mixed.cu
+struct MixedGroup;  // mixed.cu: disks of a batched sweep stepped by one launch per kernel
+struct dg_handle;
+// Grouping key of a disk ("" when it cannot join a group), group set-up, one step of the
+// whole group on a stream, and release.
+std::string mixed_group_key(const dg_handle *h);
+MixedGroup *mixed_group_create(const std::vector<dg_handle *> &disks, std::string *err);
+int mixed_group_enqueue_step(MixedGroup *g, cudaStream_t st);
+void mixed_group_destroy(MixedGroup *g);
 
 struct dg_handle {
   static constexpr int kGraphSteps = 64;  // steps per captured CUDA graph (even)

@@ -544,4 +544,60 @@ __global__ void __launch_bounds__(kThreads32t, 4) k_hydro32p(
   if (rowpend) rowtile_done(rowpend + blockIdx.y);  // this tile's outputs are written
 }
 
+// One step of a group of disks of the same grid (batched sweeps) with their own
+// self-gravity: blockIdx.z is the disk.  Each disk's fields, state tensor maps and row
+// tables come from a device array, and its tiles run exactly the single-disk kernel's
+// code (b: the ping-pong buffer that holds the input state).  The tile form below reads
+// the same entries and ignores the maps.
+struct __align__(64) HydroDisk {
+  CUtensorMap tmS[2], tmU[2], tmW[2], tmP;  // sigma, u, w of both ping-pong buffers; dPhi
+  float *sig[2], *u[2], *w[2];
+  const float *dPhi;
+  SplitBf16 Sx;
+  Ctl *ctl;
+  Rows32 g;
+};
+
+template <bool G2>
+__global__ void __launch_bounds__(kThreads32t, 4) k_hydro32p_group(const HydroDisk *__restrict__ disks, int b) {
+  extern __shared__ __align__(16) uint8_t sm32p_raw[];
+  float *sm32t = reinterpret_cast<float *>(((uintptr_t)sm32p_raw + 127) & ~(uintptr_t)127);
+  __shared__ double red[kThreads32t / 32];
+  __shared__ double bsum[2 * kMaxModes], zsum[2 * kMaxModes];
+  __shared__ __align__(8) uint64_t bar_ld, bar_rc;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&bar_ld, 1);
+    tc::mbar_init(&bar_rc, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  const HydroDisk &d = disks[blockIdx.z];
+  const int o = b ^ 1;
+  const int i0 = blockIdx.y * kTileI;
+  // the predecessor (the group's inverse phi product) writes only dPhi: early state loads
+  if (i0 >= 3 && i0 + kTileI + 3 <= d.g.Nu)
+    hydro32p_tile<G2, kForcePhi, true>(d.sig[b], d.u[b], d.w[b], d.dPhi, nullptr, nullptr, d.sig[o], d.u[o], d.w[o],
+                                       d.Sx, d.ctl, d.g, sm32t, red, bsum, zsum, &d.tmS[b], &d.tmU[b], &d.tmW[b],
+                                       &d.tmP, &bar_ld, &bar_rc, true);
+  else
+    hydro32p_tile<G2, kForcePhi, false>(d.sig[b], d.u[b], d.w[b], d.dPhi, nullptr, nullptr, d.sig[o], d.u[o], d.w[o],
+                                        d.Sx, d.ctl, d.g, sm32t, red, bsum, zsum, &d.tmS[b], &d.tmU[b], &d.tmW[b],
+                                        &d.tmP, &bar_ld, &bar_rc, true);
+}
+
+template <bool G2>
+__global__ void __launch_bounds__(kThreads32t, 4) k_hydro32t_group(const HydroDisk *__restrict__ disks, int b) {
+  extern __shared__ float sm32t[];
+  __shared__ double red[kThreads32t / 32];
+  __shared__ double bsum[2 * kMaxModes], zsum[2 * kMaxModes];
+  const HydroDisk &d = disks[blockIdx.z];
+  const int o = b ^ 1;
+  const int i0 = blockIdx.y * kTileI;
+  if (i0 >= 3 && i0 + kTileI + 3 <= d.g.Nu)
+    hydro32t_tile<G2, kForcePhi, true>(d.sig[b], d.u[b], d.w[b], d.dPhi, nullptr, nullptr, d.sig[o], d.u[o], d.w[o],
+                                       d.Sx, d.ctl, d.g, sm32t, red, bsum, zsum);
+  else
+    hydro32t_tile<G2, kForcePhi, false>(d.sig[b], d.u[b], d.w[b], d.dPhi, nullptr, nullptr, d.sig[o], d.u[o],
+                                        d.w[o], d.Sx, d.ctl, d.g, sm32t, red, bsum, zsum);
+}
+
 }  // namespace dg

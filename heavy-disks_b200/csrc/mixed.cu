@@ -1136,6 +1136,14 @@ __global__ void k_step_finalize(Ctl *ctl) {
   if (threadIdx.x == 0) finalize_launch(ctl, read_step_info(ctl, true, ctl->pend_active));
 }
 
+// the same for every disk of a group (one block per disk)
+__global__ void k_step_finalize_group(const HydroDisk *__restrict__ disks) {
+  pdl_trigger();
+  pdl_wait();
+  Ctl *ctl = disks[blockIdx.x].ctl;
+  if (threadIdx.x == 0) finalize_launch(ctl, read_step_info(ctl, true, ctl->pend_active));
+}
+
 // the step's finalisation after a tile hydro launch (the warp form finalises in its last CTA)
 static cudaError_t launch_finalize(const MixedState &X, Ctl *ctl, cudaStream_t st) {
   if (X.hydro_kind == MixedState::kHydroWarp) return cudaSuccess;
@@ -1404,3 +1412,172 @@ int dg_handle::mixed_potential(const double *dSig, double *dOut) {
   }
   return DG_OK;
 }
+
+// ---------------------------------------------------------------------------------
+// Disk groups of a batched sweep (batch.cu): disks of one grid, Gamma class, hydro form and
+// product pipeline depths advance with one launch per kernel for the whole group (the
+// disk in blockIdx.z).  Each disk keeps its own state, khat table, row tables, control
+// block and dt; the DFT tables, identical for one grid, are the lead disk's.  A disk's
+// tiles run exactly the code of its lone step, so a grouped step equals the lone one bit
+// for bit.
+
+struct MixedGroup {
+  std::vector<dg_handle *> disks;
+  dg_handle *lead = nullptr;
+  int kind = MixedState::kHydroPacked;
+  bool g2 = false;
+  int ns[6] = {0, 0, 0, 0, 0, 0};
+  tc::GemmDisk *gd[4] = {nullptr, nullptr, nullptr, nullptr};  // per product: one entry per disk
+  HydroDisk *hd = nullptr;
+};
+
+std::string mixed_group_key(const dg_handle *h) {
+  if (!h || h->p.precision != DG_PREC_MIXED || !h->p.selfgrav || !h->mx || !h->mx->tables_ready ||
+      h->mx->factored || !h->have_state)
+    return std::string();
+  const MixedState &X = *h->mx;
+  if (X.hydro_kind != MixedState::kHydroPacked && X.hydro_kind != MixedState::kHydroTile) return std::string();
+  char b[160];
+  snprintf(b, sizeof b, "%d:%d:%d:%d:%d:%d,%d,%d,%d", h->dev, X.Nu, X.Nphi, X.rows.gamma2, X.hydro_kind, X.ns[0],
+           X.ns[1], X.ns[2], X.ns[5]);
+  return std::string(b);
+}
+
+template <int MODE, bool A_MN, bool B_MN, bool PER_A>
+static cudaError_t gemm_group(const CUtensorMap &Ch, const CUtensorMap &Cl, const tc::GemmDisk *d, int G, int M,
+                              int N, int K, cudaStream_t st, int ns, bool prepare) {
+  if (M % tc::BM || N % tc::BN || K % tc::BK) return cudaErrorInvalidValue;
+  const int nk = K / tc::BK;
+  if (ns == 0) ns = nk <= 1 ? 1 : (nk <= 2 ? 2 : tc::STAGES);
+  const int NS = ns <= 1 ? 1 : (ns <= 2 ? 2 : tc::STAGES);
+  auto k1 = tc::k_gemm_split_group<MODE, A_MN, B_MN, 1, PER_A>;
+  auto k2 = tc::k_gemm_split_group<MODE, A_MN, B_MN, 2, PER_A>;
+  auto k4 = tc::k_gemm_split_group<MODE, A_MN, B_MN, tc::STAGES, PER_A>;
+  if (prepare) {
+    const void *fn = NS == 1 ? (const void *)k1 : (NS == 2 ? (const void *)k2 : (const void *)k4);
+    return smem_attrs(fn, tc::smem_bytes(NS));
+  }
+  dim3 grid(N / tc::BN, M / tc::BM, G);
+  if (NS == 1) return launch_pdl(k1, grid, dim3(tc::kThreads), tc::smem_bytes(1), st, Ch, Cl, d);
+  if (NS == 2) return launch_pdl(k2, grid, dim3(tc::kThreads), tc::smem_bytes(2), st, Ch, Cl, d);
+  return launch_pdl(k4, grid, dim3(tc::kThreads), tc::smem_bytes(tc::STAGES), st, Ch, Cl, d);
+}
+
+// The group's kernels for one step, or (prepare) the shared-memory limits they need.
+static int group_launch(MixedGroup *g, cudaStream_t st, bool prepare) {
+  dg_handle *L = g->lead;
+  MixedState &X = *L->mx;
+  const int Nu = X.Nu, Nphi = X.Nphi, G = (int)g->disks.size();
+  cudaError_t e;
+  // G1: X1[c][i] = Fphi[c][:] . Sx[i][:];  G2: Wt[c][p] = KW[c][p] X1[c][:] . Cu[p][:];
+  // G3: Z[i][c] = CuT[i][:] . Wt[c][:];    G4: dPhi[i][j] = phiscale[i] Z[i][:] . Gphi[j][:]
+  e = gemm_group<tc::kEpiSplit, false, false, false>(X.mFphi[0], X.mFphi[1], g->gd[0], G, Nphi, Nu, Nphi, st, g->ns[0],
+                                                       prepare);
+  if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: phi DFT", cudaGetErrorString(e));
+  e = gemm_group<tc::kEpiSplitScaled, false, false, true>(X.mCu[0], X.mCu[1], g->gd[1], G, Nphi, 2 * Nu, Nu, st,
+                                                          g->ns[1], prepare);
+  if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: u DFT x khat", cudaGetErrorString(e));
+  e = gemm_group<tc::kEpiSplit, false, false, false>(X.mCuT[0], X.mCuT[1], g->gd[2], G, Nu, Nphi, 2 * Nu, st,
+                                                       g->ns[2], prepare);
+  if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: inverse u DFT", cudaGetErrorString(e));
+  e = gemm_group<tc::kEpiRowScaleF32, false, false, true>(X.mGphi[0], X.mGphi[1], g->gd[3], G, Nu, Nphi, Nphi, st,
+                                                          g->ns[5], prepare);
+  if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: inverse phi DFT", cudaGetErrorString(e));
+  const bool packed = g->kind == MixedState::kHydroPacked;
+  auto hk = packed ? (g->g2 ? k_hydro32p_group<true> : k_hydro32p_group<false>)
+                   : (g->g2 ? k_hydro32t_group<true> : k_hydro32t_group<false>);
+  const size_t hsm = packed ? kSmem32p : kSmem32t;
+  if (prepare) {
+    e = smem_attrs((const void *)hk, hsm);
+    if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: hydro", cudaGetErrorString(e));
+    return DG_OK;
+  }
+  const int b = L->cur;
+  const int tj = packed ? kTileJp : kTileJ;
+  dim3 hgrid((Nphi + tj - 1) / tj, (Nu + kTileI - 1) / kTileI, G);
+  e = launch_pdl(hk, hgrid, dim3(kThreads32t), hsm, st, (const HydroDisk *)g->hd, b);
+  if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: hydro", cudaGetErrorString(e));
+  e = launch_pdl(k_step_finalize_group, dim3(G), dim3(32), 0, st, (const HydroDisk *)g->hd);
+  if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: finalisation", cudaGetErrorString(e));
+  for (dg_handle *h : g->disks) h->cur ^= 1;
+  return DG_OK;
+}
+
+void mixed_group_destroy(MixedGroup *g) {
+  if (!g) return;
+  for (tc::GemmDisk *p : g->gd)
+    if (p) cudaFree(p);
+  if (g->hd) cudaFree(g->hd);
+  delete g;
+}
+
+MixedGroup *mixed_group_create(const std::vector<dg_handle *> &disks, std::string *err) {
+  if (disks.empty()) return nullptr;
+  const std::string key = mixed_group_key(disks[0]);
+  for (dg_handle *h : disks)
+    if (key.empty() || mixed_group_key(h) != key || h->cur != disks[0]->cur) {
+      *err = "batch group: disks differ in grid, Gamma class, hydro form or buffer parity";
+      return nullptr;
+    }
+  MixedGroup *g = new MixedGroup();
+  g->disks = disks;
+  g->lead = disks[0];
+  const MixedState &XL = *g->lead->mx;
+  g->kind = XL.hydro_kind;
+  g->g2 = XL.rows.gamma2 != 0;
+  for (int k = 0; k < 6; ++k) g->ns[k] = XL.ns[k];
+  const int G = (int)disks.size(), Nu = XL.Nu, Nphi = XL.Nphi;
+  std::vector<tc::GemmDisk> gd[4];
+  std::vector<HydroDisk> hd(G);
+  for (int q = 0; q < 4; ++q) gd[q].resize(G);
+  for (int k = 0; k < G; ++k) {
+    dg_handle *h = disks[k];
+    MixedState &X = *h->mx;
+    tc::GemmArgs a{};
+    a.status = &h->ctl->status;
+    // G1: per-disk B = Sx -> X1
+    a.M = Nphi; a.N = Nu; a.K = Nphi; a.out_hi = X.X1.hi; a.out_lo = X.X1.lo; a.ldo = Nu;
+    gd[0][k].hi = X.mSx[0]; gd[0][k].lo = X.mSx[1]; gd[0][k].args = a;
+    // G2: per-disk A = X1 -> Wt, x KW
+    a.M = Nphi; a.N = 2 * Nu; a.K = Nu; a.out_hi = X.Wt.hi; a.out_lo = X.Wt.lo; a.ldo = 2 * Nu; a.table = X.KW;
+    gd[1][k].hi = X.mX1[0]; gd[1][k].lo = X.mX1[1]; gd[1][k].args = a;
+    // G3: per-disk B = Wt -> Z
+    a.M = Nu; a.N = Nphi; a.K = 2 * Nu; a.out_hi = X.Z.hi; a.out_lo = X.Z.lo; a.ldo = Nphi; a.table = nullptr;
+    gd[2][k].hi = X.mWt[0]; gd[2][k].lo = X.mWt[1]; gd[2][k].args = a;
+    // G4: per-disk A = Z -> dPhi (FP32, scaled by -G du dphi / sqrt(R))
+    a.M = Nu; a.N = Nphi; a.K = Nphi; a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi;
+    a.row_scale = X.phiscale;
+    gd[3][k].hi = X.mZ[0]; gd[3][k].lo = X.mZ[1]; gd[3][k].args = a;
+    HydroDisk &d = hd[k];
+    for (int b = 0; b < 2; ++b) {
+      d.tmS[b] = X.mSig[b]; d.tmU[b] = X.mU[b]; d.tmW[b] = X.mW[b];
+      d.sig[b] = X.sig[b]; d.u[b] = X.u[b]; d.w[b] = X.w[b];
+    }
+    d.tmP = X.mPhi;
+    d.dPhi = X.dPhi;
+    d.Sx = SplitBf16{X.Sx.hi, X.Sx.lo};
+    d.ctl = h->ctl;
+    d.g = X.rows;
+  }
+  cudaError_t e = cudaSetDevice(g->lead->dev);
+  for (int q = 0; q < 4 && e == cudaSuccess; ++q) {
+    e = cudaMalloc(&g->gd[q], sizeof(tc::GemmDisk) * G);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(g->gd[q], gd[q].data(), sizeof(tc::GemmDisk) * G, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&g->hd, sizeof(HydroDisk) * G);
+  if (e == cudaSuccess) e = cudaMemcpy(g->hd, hd.data(), sizeof(HydroDisk) * G, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    *err = std::string("batch group tables: ") + cudaGetErrorString(e);
+    mixed_group_destroy(g);
+    return nullptr;
+  }
+  if (group_launch(g, nullptr, true) != DG_OK) {
+    *err = g->lead->err;
+    mixed_group_destroy(g);
+    return nullptr;
+  }
+  return g;
+}
+
+int mixed_group_enqueue_step(MixedGroup *g, cudaStream_t st) { return group_launch(g, st, false); }

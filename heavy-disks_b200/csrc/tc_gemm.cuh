@@ -291,10 +291,10 @@ __device__ __forceinline__ void epi_factored(const GemmArgs &a, int row, int col
   }
 }
 
-template <int MODE, bool A_MN = false, bool B_MN = false, int NS = STAGES>
-__global__ void __launch_bounds__(kThreads, (NS == 1 ? 4 : (NS == 2 ? 2 : 1)))
-    k_gemm_split(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
-                 const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, GemmArgs args) {
+// The body of one CTA tile (blockIdx.x: N tile, blockIdx.y: M tile) of the split GEMM.
+template <int MODE, bool A_MN, bool B_MN, int NS>
+__device__ __forceinline__ void gemm_tile(const CUtensorMap *pAh, const CUtensorMap *pAl, const CUtensorMap *pBh,
+                                          const CUtensorMap *pBl, const GemmArgs &args) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ __align__(8) uint64_t full_bar[NS], empty_bar[NS], done_bar;
@@ -337,20 +337,20 @@ __global__ void __launch_bounds__(kThreads, (NS == 1 ? 4 : (NS == 2 ? 2 : 1)))
       uint8_t *st = smem + s * kStageBytes;
       mbar_arrive_expect_tx(&full_bar[s], kStageBytes);
       if (A_MN) {  // [K][M] in global: two 64-wide M chunks of 64 K rows
-        tma_load_2d(st, &tmAh, &full_bar[s], m0, kc * BK);
-        tma_load_2d(st + kTileA / 2, &tmAh, &full_bar[s], m0 + 64, kc * BK);
-        tma_load_2d(st + kTileA, &tmAl, &full_bar[s], m0, kc * BK);
-        tma_load_2d(st + kTileA + kTileA / 2, &tmAl, &full_bar[s], m0 + 64, kc * BK);
+        tma_load_2d(st, pAh, &full_bar[s], m0, kc * BK);
+        tma_load_2d(st + kTileA / 2, pAh, &full_bar[s], m0 + 64, kc * BK);
+        tma_load_2d(st + kTileA, pAl, &full_bar[s], m0, kc * BK);
+        tma_load_2d(st + kTileA + kTileA / 2, pAl, &full_bar[s], m0 + 64, kc * BK);
       } else {
-        tma_load_2d(st, &tmAh, &full_bar[s], kc * BK, m0);
-        tma_load_2d(st + kTileA, &tmAl, &full_bar[s], kc * BK, m0);
+        tma_load_2d(st, pAh, &full_bar[s], kc * BK, m0);
+        tma_load_2d(st + kTileA, pAl, &full_bar[s], kc * BK, m0);
       }
       if (B_MN) {  // [K][N] in global: one 64-wide N chunk
-        tma_load_2d(st + 2 * kTileA, &tmBh, &full_bar[s], n0, kc * BK);
-        tma_load_2d(st + 2 * kTileA + kTileB, &tmBl, &full_bar[s], n0, kc * BK);
+        tma_load_2d(st + 2 * kTileA, pBh, &full_bar[s], n0, kc * BK);
+        tma_load_2d(st + 2 * kTileA + kTileB, pBl, &full_bar[s], n0, kc * BK);
       } else {
-        tma_load_2d(st + 2 * kTileA, &tmBh, &full_bar[s], kc * BK, n0);
-        tma_load_2d(st + 2 * kTileA + kTileB, &tmBl, &full_bar[s], kc * BK, n0);
+        tma_load_2d(st + 2 * kTileA, pBh, &full_bar[s], kc * BK, n0);
+        tma_load_2d(st + 2 * kTileA + kTileB, pBl, &full_bar[s], kc * BK, n0);
       }
       ++issued;
     }
@@ -442,6 +442,34 @@ __global__ void __launch_bounds__(kThreads, (NS == 1 ? 4 : (NS == 2 ? 2 : 1)))
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem_d, kTmemCols);
+}
+
+template <int MODE, bool A_MN = false, bool B_MN = false, int NS = STAGES>
+__global__ void __launch_bounds__(kThreads, (NS == 1 ? 4 : (NS == 2 ? 2 : 1)))
+    k_gemm_split(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
+                 const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl, GemmArgs args) {
+  gemm_tile<MODE, A_MN, B_MN, NS>(&tmAh, &tmAl, &tmBh, &tmBl, args);
+}
+
+// One product for a group of disks of the same grid (batched sweeps): blockIdx.z is the
+// disk.  One operand is the group's shared DFT table (the grid-constant maps), the other
+// is the disk's own (its tensor maps sit with its epilogue arguments in a device array;
+// TMA reads a map from global memory as from a kernel parameter).  PER_A: the per-disk
+// operand is A.  Each disk's tiles run exactly the single-disk kernel's code.
+struct __align__(64) GemmDisk {
+  CUtensorMap hi, lo;  // the disk's operand (hi / lo planes)
+  GemmArgs args;       // its epilogue: outputs, khat table, row scale, status word
+};
+
+template <int MODE, bool A_MN, bool B_MN, int NS, bool PER_A>
+__global__ void __launch_bounds__(kThreads, (NS == 1 ? 4 : (NS == 2 ? 2 : 1)))
+    k_gemm_split_group(const __grid_constant__ CUtensorMap tmCh, const __grid_constant__ CUtensorMap tmCl,
+                       const GemmDisk *__restrict__ disks) {
+  const GemmDisk &d = disks[blockIdx.z];
+  if (PER_A)
+    gemm_tile<MODE, A_MN, B_MN, NS>(&d.hi, &d.lo, &tmCh, &tmCl, d.args);
+  else
+    gemm_tile<MODE, A_MN, B_MN, NS>(&tmCh, &tmCl, &d.hi, &d.lo, d.args);
 }
 
 }  // namespace tc

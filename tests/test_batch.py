@@ -37,3 +37,33 @@ def test_batch_equals_individual_runs(precision):
             assert np.array_equal(a, c)
         assert recs[k].shape == rec1.shape
         assert np.allclose(recs[k], rec1, rtol=1e-12, atol=1e-15)
+
+
+def test_grouped_batch_equals_ungrouped_and_lone(monkeypatch):
+    """16 sweep disks over all four sweep grids plus two plain FP64 disks: the mixed disks
+    form same-grid groups advanced by one launch per kernel (blockIdx.z = disk); the result
+    is bit for bit the one with grouping off (DISKGPU_BATCH_GROUPS=0, one graph branch per
+    disk) and the one of lone runs."""
+    pts = S.draw(16, seed=3, grids=(128, 256, 384, 512))
+    params = [_params(p, "mixed") for p in pts] + [_params(p, "fp64") for p in pts[:2]]
+    tlim = 0.03
+    out = {}
+    for grouped in ("1", "0"):
+        monkeypatch.setenv("DISKGPU_BATCH_GROUPS", grouped)
+        with D.Batch(params) as b:
+            b.init_standard()
+            recs, t, steps = b.advance(tlim, steps_per_launch=8, dtout=0.01)
+            out[grouped] = ([d.get_state() for d in b.disks], recs, t, steps)
+    (sa, ra, ta, na), (sb, rb, tb, nb) = out["1"], out["0"]
+    assert np.array_equal(na, nb) and np.array_equal(ta, tb)
+    for k in range(len(params)):
+        for x, y in zip(sa[k], sb[k]):
+            assert np.array_equal(x, y), k
+        np.testing.assert_array_equal(ra[k], rb[k])
+    for k in (0, 5, 16):
+        p = params[k]
+        with D.Disk(p.Nu, p.Nphi, params=p, precision="mixed" if p.precision == D.MIXED else "fp64") as d:
+            d.init_standard()
+            d.advance(tlim, dtout=0.01)
+            for x, y in zip(sa[k], d.get_state()):
+                assert np.array_equal(x, y), k
