@@ -76,6 +76,9 @@ def parse():
                     help="steps of the plain FP64 path on the same disk (default: --steps; 0: skip it)")
     ap.add_argument("--repeats", type=int, default=5, help="extra timed regions of K steps for the spread")
     ap.add_argument("--cufft", type=int, default=1, help="time the cuFFT form of the gravity (0: skip)")
+    ap.add_argument("--drift-steps", type=int, default=0,
+                    help="steps with the per-step m = 0..8 diagnostic on, reporting the FP64 mass and angular "
+                         "momentum drift (0: skip)")
     ap.add_argument("--batch-disks", type=int, default=256,
                     help="disks of the batched sweep measurement (0: skip it)")
     ap.add_argument("--batch-tlim", type=float, default=0.1, help="time the batched sweep advances")
@@ -400,20 +403,17 @@ def cufft_gravity(a, device, flush, disk64_potential):
     return out
 
 
-def batched_sweep(a, device):
+def batched_sweep(a, device, grouped=True):
     """Throughput of a batched sweep: `--batch-disks` disks drawn by the sweep law (grids
     128^2..512^2, Q_min, M_d/M_*, softening/r, Gamma; seed 12345), mixed precision, advanced
-    together by dg_batch (one graph launch advances every disk 64 steps)."""
+    together by dg_batch (one graph launch advances every disk 64 steps; same-grid disks
+    as groups, one launch per kernel, unless grouped is False)."""
     import torch
     import diskgpu as D
     from diskgpu import sweep as S
+    os.environ["DISKGPU_BATCH_GROUPS"] = "1" if grouped else "0"
     pts = S.draw(a.batch_disks, seed=12345, grids=(128, 256, 384, 512))
-    params = []
-    for pt in pts:
-        p, _ = D.params_physical(pt.Qmin, pt.mass_ratio, pt.soft_over_r, pt.gamma)
-        p.Nu = p.Nphi = pt.N
-        p.amp, p.phase0, p.precision, p.device = 1e-3, pt.phase0, D.MIXED, device
-        params.append(p)
+    params = [S.point_params(pt, "mixed", device) for pt in pts]
     with D.Batch(params) as b:
         b.init_standard()
         _, _, s0 = b.advance(0.01, steps_per_launch=64)  # captures the graph
@@ -421,14 +421,23 @@ def batched_sweep(a, device):
         t0 = time.perf_counter()
         _, _, s1 = b.advance(0.01 + a.batch_tlim, steps_per_launch=64)
         el = time.perf_counter() - t0
+    os.environ.pop("DISKGPU_BATCH_GROUPS", None)
     zu = float(sum(pt.N * pt.N * (int(x1) - int(x0)) for pt, x0, x1 in zip(pts, s0, s1)))
+    # split-BF16 dense DFT products of a disk step: 6 N^3 (phi) + 12 N^3 + 12 N^3 (u) + 6 N^3 (inverse phi)
+    flops = float(sum(36.0 * pt.N ** 3 * (int(x1) - int(x0)) for pt, x0, x1 in zip(pts, s0, s1)))
     grids = {}
     for pt in pts:
         grids[pt.N] = grids.get(pt.N, 0) + 1
+    hbm_peak, tc_peak, kind = measured_peaks()
+    hyd = 32.0 * zu / el / 1e9
     return {"value": zu / el, "unit": UNIT, "disks": len(pts), "grids": {f"{k}^2": v for k, v in sorted(grids.items())},
-            "zone_updates": zu, "seconds": el, "sim_time": a.batch_tlim,
+            "zone_updates": zu, "seconds": el, "sim_time": a.batch_tlim, "grouped": grouped,
+            "hydro_algorithmic_GBps": hyd, "hydro_frac_of_hbm": hyd / hbm_peak,
+            "gravity_executed_TFLOPs": flops / el / 1e12, "gravity_frac_of_tensor": flops / el / 1e12 / tc_peak,
+            "peak_kind": kind,
             "how": "wall clock around dg_batch_advance (graph launches of 64 steps per disk, the host reads "
-                   "every disk's control block between launches)"}
+                   "every disk's control block between launches); algorithmic rates over the whole job: 32 B per "
+                   "zone-update for the hydro, 36 N^3 executed flops per disk-step for the dense gravity products"}
 
 
 TRAFFIC_KEYS = {"hydro": "hydro", "grav_phi_fwd": "grav_phi_fwd", "grav_u": "grav_u", "grav_phi_inv": "grav_phi_inv"}
@@ -494,6 +503,25 @@ def main():
     disk.run_steps(0, 0.3, sync=True)  # surfaces any device-side error of the timed steps
     zones = N * N
     value = world * zones * a.steps / (ms_max * 1e-3)
+
+    # ---- optional: per-step m = 0..8 diagnostics and the drift of the FP64 global sums ----
+    drift = None
+    if a.drift_steps > 0:
+        disk.set_diagnostics(8, a.drift_steps + 8)
+        m0, L0 = disk.conserved()
+        with torch.cuda.stream(stream):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            disk.run_steps(a.drift_steps, 0.3, sync=False)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        m1, L1 = disk.conserved()
+        tdg, Cdg = disk.diagnostics()
+        disk.set_diagnostics(8, 0)
+        drift = {"steps": a.drift_steps, "rows": int(len(tdg)), "ms_per_step_with_diagnostics":
+                 e0.elapsed_time(e1) / a.drift_steps, "mass_rel_drift": (m1 - m0) / m0,
+                 "angmom_rel_drift": (L1 - L0) / L0, "C0_max_dev": float(np.max(np.abs(Cdg[:, 0] - 1.0))),
+                 "C2_abs_last": float(abs(Cdg[-1, 2])) if len(Cdg) else None}
 
     # ---- single steps with a cold L2 (flushed before each), then the per-kernel split ----
     cold_n = max(1, min(a.cold_steps, a.steps))
@@ -600,7 +628,8 @@ def main():
                              f"{2 * N}x{N} convolution, graph-replayed after an L2 flush; tcgen05_gravity_ms = the "
                              "mixed step's three gravity kernels, each timed alone after an L2 flush")
         if a.batch_disks > 0:
-            batch = batched_sweep(a, local)
+            batch = batched_sweep(a, local, grouped=True)
+            batch["ungrouped"] = batched_sweep(a, local, grouped=False)["value"]
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -627,7 +656,7 @@ def main():
             "roofline": roof, "roofline_all": roof_all, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": kps * a.steps, "clocks": clk.summary(),
             "repeats": spread(reps, a.steps) if reps else None,
-            "fp64_same_disk": fp64, "cufft_gravity": cufft, "batched_sweep": batch,
+            "fp64_same_disk": fp64, "cufft_gravity": cufft, "batched_sweep": batch, "conservation": drift,
         }
         print(json.dumps(line))
     disk.close()

@@ -221,25 +221,29 @@ __device__ __forceinline__ void hydro32p_tile(
     return;
   }
 
-  // ---- S1: pressure perturbation dP of the staged rows ----
+  // pressure perturbation dP = K s (2 Sigma0 + s) for Gamma = 2 (zero outside the grid,
+  // where the staged s and the tabulated Sigma0 are zero)
+  auto dp2 = [&](F2 s, float s0) { return mul(mul(S(g.Kpoly), s), add(S(2.f * s0), s)); };
+
+  // ---- S1 (Gamma != 2): pressure perturbation dP of the staged rows; for Gamma = 2 the
+  // source stage evaluates it where it needs it (three cheap products per point), so there
+  // is no separate stage and barrier ----
+  if (!G2) {
 #pragma unroll
-  for (int k = 0; k < kItLoadP; ++k) {
-    const int r = wp + kWarps32p * k, i = ib + r;
-    if (r < kRows32t) {
-      const F2 s = SG[r * L2 + lane];
-      F2 d = S(0.f);
-      if (row_ok(i)) {
-        if (G2) {
-          d = mul(mul(S(g.Kpoly), s), add(S(2.f * RC(tS0, i)), s));
-        } else {
+    for (int k = 0; k < kItLoadP; ++k) {
+      const int r = wp + kWarps32p * k, i = ib + r;
+      if (r < kRows32t) {
+        const F2 s = SG[r * L2 + lane];
+        F2 d = S(0.f);
+        if (row_ok(i)) {
           const float P0 = RC(tP0, i), iS0 = RC(tInvS0, i);
           d = make_float2(P0 * expm1f(g.gamma * log1pf(s.x * iS0)), P0 * expm1f(g.gamma * log1pf(s.y * iS0)));
         }
+        DP[r * L2 + lane] = d;
       }
-      DP[r * L2 + lane] = d;
     }
+    __syncthreads();
   }
-  __syncthreads();
 
   // ---- S2: source kick of rows i0-2 .. i0+kTileI+1 (hydro.hpp:73-96) ----
 #pragma unroll
@@ -247,7 +251,7 @@ __device__ __forceinline__ void hydro32p_tile(
     const int rs = wp + kWarps32p * k, r = rs + 1, i = ib + r;
     if (rs < kSrcRows32t) {  // warp-uniform
       const int x = r * L2 + lane;
-      const F2 dc = DP[x];
+      const F2 dc = G2 ? dp2(SG[x], RC(tS0, i)) : DP[x];
       // azimuthal neighbours: column 2l-1 is the left lane's .y, 2l+2 the right lane's .x
       const float dl = up1(dc.y), dr = dn1(dc.x);
       F2 pc = S(0.f);
@@ -262,8 +266,8 @@ __device__ __forceinline__ void hydro32p_tile(
         const float4 c0 = RC4(0, i), c1 = RC4(1, i);  // S0 invS0 V0 a0 | dP0/dR invdRc invR R
         const F2 s_g = SG[x];
         const F2 s = add(S(c0.x), s_g);
-        const F2 pim = first_row(i) ? dc : DP[x - L2];
-        const F2 pip = last_row(i) ? dc : DP[x + L2];
+        const F2 pim = first_row(i) ? dc : (G2 ? dp2(SG[x - L2], RC(tS0, i - 1)) : DP[x - L2]);
+        const F2 pip = last_row(i) ? dc : (G2 ? dp2(SG[x + L2], RC(tS0, i + 1)) : DP[x + L2]);
         const F2 ddP = mul(sub(pip, pim), S(c1.y));
         const F2 dPdphi = mul(sub(make_float2(dc.y, dr), make_float2(dl, dc.x)), S(g.inv2dphi));
         const float iR = c1.z;
