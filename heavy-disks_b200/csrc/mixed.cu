@@ -190,6 +190,11 @@ static bool make_map(CUtensorMap *m, const void *base, uint64_t rows, uint64_t c
   return r == CUDA_SUCCESS;
 }
 
+// the same map for other files of the library (the surrogate network's operands)
+bool dg_bf16_tensor_map(CUtensorMap *m, const void *base, uint64_t rows, uint64_t cols, uint32_t box_rows) {
+  return make_map(m, base, rows, cols, box_rows);
+}
+
 // ---------------------------------------------------------------------------------
 // DFT tables (built on the device in FP64, stored as BF16 pairs)
 

@@ -43,6 +43,11 @@ enum EpiMode : int {
   kEpiTwiddleF1 = 4,    // rows (p2, ri), cols (m, i1): x W_M^{p2 i1} -> T[(i1, ri)][(m, p2)]
   kEpiTwiddleI1 = 5,    // rows (m, p2), cols (i1, ri): x W_M^{-p2 i1} -> U[(m, i1)][(p2, ri)]
   kEpiI2ToZ = 6,        // rows (m, i1), cols (i2, ri) -> Z[c(m, ri)][i1 + A i2]
+  // surrogate network (mlp.cu); row stride ldo everywhere
+  kEpiMlpAct = 7,       // z = D + bias[col] -> out_f32 (pre-activation); split(SiLU(z)) -> out_hi / out_lo
+  kEpiMlpOut = 8,       // D + bias[col] -> out_f32 (linear head)
+  kEpiMlpBack = 9,      // d = D * SiLU'(table[row][col]) -> out_f32 and split(d) -> out_hi / out_lo
+  kEpiStoreBounded = 10,  // D -> out_f32[row][col] for row < lim_m, col < lim_n (weight gradients)
 };
 
 struct GemmArgs {
@@ -60,6 +65,9 @@ struct GemmArgs {
   // sets rowpend[0 .. rp_n) = rp_val once this kernel's predecessor has completed
   int *rowpend;
   int rp_n, rp_val;
+  // surrogate network epilogues
+  const float *bias;   // kEpiMlpAct, kEpiMlpOut: per column, padded with zeros
+  int lim_m, lim_n;    // kEpiStoreBounded
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -291,6 +299,64 @@ __device__ __forceinline__ void epi_factored(const GemmArgs &a, int row, int col
   }
 }
 
+// Epilogues of the surrogate network's products: 32 accumulator columns from col of one row.
+__device__ __forceinline__ float silu_f(float z) { return z / (1.f + __expf(-z)); }
+__device__ __forceinline__ float silu_grad_f(float z) {
+  const float sg = 1.f / (1.f + __expf(-z));
+  return sg * (1.f + z * (1.f - sg));
+}
+
+template <int MODE>
+__device__ __forceinline__ void epi_mlp_bounded(const GemmArgs &a, int row, int col, const uint32_t (&r)[32]) {
+  if (row >= a.lim_m) return;
+  const size_t base = (size_t)row * a.ldo + col;
+#pragma unroll
+  for (int q = 0; q < 32; ++q)
+    if (col + q < a.lim_n) a.out_f32[base + q] = __uint_as_float(r[q]);
+}
+
+template <int MODE>
+__device__ __forceinline__ void epi_mlp(const GemmArgs &a, int row, int col, const uint32_t (&r)[32]) {
+  const size_t base = (size_t)row * a.ldo + col;
+  float v[32];
+#pragma unroll
+  for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
+  if (MODE == kEpiMlpAct || MODE == kEpiMlpOut) {
+#pragma unroll
+    for (int q = 0; q < 32; ++q) v[q] += __ldg(a.bias + col + q);
+  }
+  if (MODE == kEpiMlpBack) {
+    const float *z = a.table + base;
+#pragma unroll
+    for (int q = 0; q < 32; ++q) v[q] *= silu_grad_f(z[q]);
+  }
+  float4 *o = reinterpret_cast<float4 *>(a.out_f32 + base);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  if (MODE == kEpiMlpAct || MODE == kEpiMlpBack) {
+    if (MODE == kEpiMlpAct) {
+#pragma unroll
+      for (int q = 0; q < 32; ++q) v[q] = silu_f(v[q]);
+    }
+    uint32_t ph[16], pl[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      __nv_bfloat16 h0, l0, h1, l1;
+      split_bf16(v[2 * q], h0, l0);
+      split_bf16(v[2 * q + 1], h1, l1);
+      ph[q] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+      pl[q] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+    }
+    uint4 *oh = reinterpret_cast<uint4 *>(a.out_hi + base);
+    uint4 *ol = reinterpret_cast<uint4 *>(a.out_lo + base);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      oh[q] = make_uint4(ph[4 * q], ph[4 * q + 1], ph[4 * q + 2], ph[4 * q + 3]);
+      ol[q] = make_uint4(pl[4 * q], pl[4 * q + 1], pl[4 * q + 2], pl[4 * q + 3]);
+    }
+  }
+}
+
 // The body of one CTA tile (blockIdx.x: N tile, blockIdx.y: M tile) of the split GEMM.
 template <int MODE, bool A_MN, bool B_MN, int NS>
 __device__ __forceinline__ void gemm_tile(const CUtensorMap *pAh, const CUtensorMap *pAl, const CUtensorMap *pBh,
@@ -397,6 +463,14 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap *pAh, const CUtensor
       uint32_t r[32];
       tmem_ld32(tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
       const int col = n0 + c0;
+      if (MODE == kEpiStoreBounded) {
+        epi_mlp_bounded<MODE>(args, row, col, r);
+        continue;
+      }
+      if (MODE >= kEpiMlpAct) {
+        epi_mlp<MODE>(args, row, col, r);
+        continue;
+      }
       if (MODE >= kEpiPhiToXin) {
         epi_factored<MODE>(args, row, col, r, lane);
         continue;
