@@ -41,9 +41,10 @@ def test_batch_equals_individual_runs(precision):
 
 def test_grouped_batch_equals_ungrouped_and_lone(monkeypatch):
     """16 sweep disks over all four sweep grids plus two plain FP64 disks: the mixed disks
-    form same-grid groups advanced by one launch per kernel (blockIdx.z = disk); the result
-    is bit for bit the one with grouping off (DISKGPU_BATCH_GROUPS=0, one graph branch per
-    disk) and the one of lone runs."""
+    form same-grid groups advanced by one launch per kernel (blockIdx.z = disk); the states
+    are bit for bit the ones with grouping off (DISKGPU_BATCH_GROUPS=0, one graph branch
+    per disk) and the ones of lone runs, the step counts and times equal; the mode records
+    agree to 1e-12 (their FP64 sums are folded with atomics in a varying order)."""
     pts = S.draw(16, seed=3, grids=(128, 256, 384, 512))
     params = [_params(p, "mixed") for p in pts] + [_params(p, "fp64") for p in pts[:2]]
     tlim = 0.03
@@ -59,7 +60,7 @@ def test_grouped_batch_equals_ungrouped_and_lone(monkeypatch):
     for k in range(len(params)):
         for x, y in zip(sa[k], sb[k]):
             assert np.array_equal(x, y), k
-        np.testing.assert_array_equal(ra[k], rb[k])
+        np.testing.assert_allclose(ra[k], rb[k], rtol=1e-12, atol=1e-15)
     for k in (0, 5, 16):
         p = params[k]
         with D.Disk(p.Nu, p.Nphi, params=p, precision="mixed" if p.precision == D.MIXED else "fp64") as d:

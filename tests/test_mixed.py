@@ -136,7 +136,7 @@ def test_4096_disk_conservation_and_diagnostics():
     assert len(t) == 300 and C.shape == (300, 9)
     assert np.all(np.diff(t) > 0)
     assert np.max(np.abs(C[:, 0] - 1.0)) < 1e-9
-    assert abs(C[-1, 2]) > 0.5e-3  # the m = 2 seed is carried
+    assert abs(C[-1, 2]) > 4e-4  # the m = 2 seed (|C2| = amp / 2 = 5e-4) is carried
     assert abs(m1 - m0) <= 1e-11 * m0, (m1 - m0) / m0
     assert abs(L1 - L0) <= 1e-8 * abs(L0), (L1 - L0) / L0
 
@@ -295,7 +295,10 @@ def test_capture_graph_up_front_changes_nothing(monkeypatch):
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_advance_with_record_callback_matches_advance(prec):
-    """dg_advance_cb hands over the same records, in order, as dg_advance collects."""
+    """dg_advance_cb hands over the same records, in order, as dg_advance collects: the
+    same times and step counts, the records of one run exactly as the callback saw them,
+    and those of two runs to 1e-12 (each CTA folds its share of the mode sums with an FP64
+    atomic add, so the summation order, and the last bits, vary between runs)."""
     runs = []
     for cb in (False, True):
         seen = []
@@ -305,5 +308,5 @@ def test_advance_with_record_callback_matches_advance(prec):
         runs.append((rec, t, n))
         if cb:
             np.testing.assert_array_equal(np.array(seen), rec)
-    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    np.testing.assert_allclose(runs[0][0], runs[1][0], rtol=1e-12, atol=1e-15)
     assert runs[0][1:] == runs[1][1:]
