@@ -1,7 +1,7 @@
 // Batched sweeps: many independent disks (heterogeneous grids and parameters) advanced
 // together by one CUDA graph per launch.  Mixed-precision disks that share a grid, a
-// Gamma class (Gamma = 2 or not), a hydro kernel form and product pipeline depths form a
-// group: one launch per kernel advances the whole group (mixed.cu, disk groups), the disk
+// Gamma class (Gamma = 2 or not), a hydro kernel form, product pipeline depths and a step
+// rate within a factor 2^(1/4) form a group: one launch per kernel advances the whole group (mixed.cu, disk groups), the disk
 // in blockIdx.z.  Every other disk is a branch of its own, holding its single-disk steps.
 // The graph forks one branch per group or lone disk from a root stream, each on its own
 // stream, so the branches overlap on the GPU, and joins back.  Every disk keeps its own
@@ -160,9 +160,16 @@ int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int ste
       const bool grouping = !(ge && strcmp(ge, "0") == 0);
       std::map<std::string, std::vector<int>> by_key;
       for (int k = 0; k < n; ++k) {
-        const std::string key = grouping ? mixed_group_key(b->disks[k]) : std::string();
-        if (key.empty()) branches.emplace_back(1, k);
-        else by_key[key].push_back(k);
+        std::string key = grouping ? mixed_group_key(b->disks[k]) : std::string();
+        if (key.empty()) {
+          branches.emplace_back(1, k);
+          continue;
+        }
+        // step-rate class: a group's disks all take the group's (largest) step count per
+        // launch, so members are within a factor 2^(1/4) of each other's rate and few of
+        // their steps are pass-throughs
+        key += ":" + std::to_string((int)std::floor(4.0 * std::log2((double)b->steps_per_launch[k])));
+        by_key[key].push_back(k);
       }
       for (auto &kv : by_key) {
         if (kv.second.size() == 1) {

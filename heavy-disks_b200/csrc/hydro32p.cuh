@@ -70,6 +70,10 @@ __device__ __forceinline__ F2 sels(bool px, bool py, float a, float b) {
   return make_float2(px ? a : b, py ? a : b);
 }
 __device__ __forceinline__ F2 fdiv(F2 a, F2 b) { return make_float2(__fdividef(a.x, b.x), __fdividef(a.y, b.y)); }
+// the fast divide is a * (1 / b), so several quotients by one b share one reciprocal
+__device__ __forceinline__ F2 rcp(F2 b) { return make_float2(__fdividef(1.f, b.x), __fdividef(1.f, b.y)); }
+// sqrt(x) for x > 0 as x rsqrt(x): one special-function operation
+__device__ __forceinline__ float sqrt_pos(float x) { return x * rsqrtf(x); }
 // hydro.hpp:16-18 on each half (see vanleer32)
 __device__ __forceinline__ F2 vanleer(F2 a, F2 b) {
   const F2 p = mul(a, b), s = add(a, b), n = add(p, p);
@@ -221,29 +225,25 @@ __device__ __forceinline__ void hydro32p_tile(
     return;
   }
 
-  // pressure perturbation dP = K s (2 Sigma0 + s) for Gamma = 2 (zero outside the grid,
-  // where the staged s and the tabulated Sigma0 are zero)
-  auto dp2 = [&](F2 s, float s0) { return mul(mul(S(g.Kpoly), s), add(S(2.f * s0), s)); };
-
-  // ---- S1 (Gamma != 2): pressure perturbation dP of the staged rows; for Gamma = 2 the
-  // source stage evaluates it where it needs it (three cheap products per point), so there
-  // is no separate stage and barrier ----
-  if (!G2) {
+  // ---- S1: pressure perturbation dP of the staged rows ----
 #pragma unroll
-    for (int k = 0; k < kItLoadP; ++k) {
-      const int r = wp + kWarps32p * k, i = ib + r;
-      if (r < kRows32t) {
-        const F2 s = SG[r * L2 + lane];
-        F2 d = S(0.f);
-        if (row_ok(i)) {
+  for (int k = 0; k < kItLoadP; ++k) {
+    const int r = wp + kWarps32p * k, i = ib + r;
+    if (r < kRows32t) {
+      const F2 s = SG[r * L2 + lane];
+      F2 d = S(0.f);
+      if (row_ok(i)) {
+        if (G2) {
+          d = mul(mul(S(g.Kpoly), s), add(S(2.f * RC(tS0, i)), s));
+        } else {
           const float P0 = RC(tP0, i), iS0 = RC(tInvS0, i);
           d = make_float2(P0 * expm1f(g.gamma * log1pf(s.x * iS0)), P0 * expm1f(g.gamma * log1pf(s.y * iS0)));
         }
-        DP[r * L2 + lane] = d;
       }
+      DP[r * L2 + lane] = d;
     }
-    __syncthreads();
   }
+  __syncthreads();
 
   // ---- S2: source kick of rows i0-2 .. i0+kTileI+1 (hydro.hpp:73-96) ----
 #pragma unroll
@@ -251,7 +251,7 @@ __device__ __forceinline__ void hydro32p_tile(
     const int rs = wp + kWarps32p * k, r = rs + 1, i = ib + r;
     if (rs < kSrcRows32t) {  // warp-uniform
       const int x = r * L2 + lane;
-      const F2 dc = G2 ? dp2(SG[x], RC(tS0, i)) : DP[x];
+      const F2 dc = DP[x];
       // azimuthal neighbours: column 2l-1 is the left lane's .y, 2l+2 the right lane's .x
       const float dl = up1(dc.y), dr = dn1(dc.x);
       F2 pc = S(0.f);
@@ -266,8 +266,8 @@ __device__ __forceinline__ void hydro32p_tile(
         const float4 c0 = RC4(0, i), c1 = RC4(1, i);  // S0 invS0 V0 a0 | dP0/dR invdRc invR R
         const F2 s_g = SG[x];
         const F2 s = add(S(c0.x), s_g);
-        const F2 pim = first_row(i) ? dc : (G2 ? dp2(SG[x - L2], RC(tS0, i - 1)) : DP[x - L2]);
-        const F2 pip = last_row(i) ? dc : (G2 ? dp2(SG[x + L2], RC(tS0, i + 1)) : DP[x + L2]);
+        const F2 pim = first_row(i) ? dc : DP[x - L2];
+        const F2 pip = last_row(i) ? dc : DP[x + L2];
         const F2 ddP = mul(sub(pip, pim), S(c1.y));
         const F2 dPdphi = mul(sub(make_float2(dc.y, dr), make_float2(dl, dc.x)), S(g.inv2dphi));
         const float iR = c1.z;
@@ -286,9 +286,10 @@ __device__ __forceinline__ void hydro32p_tile(
         }
         const F2 uc = U0[x], wc = W0[x];  // raw u, w of the point (row r of the staged fields)
         const float V = c0.z;
-        const F2 q1 = fdiv(sub(mul(mul(S(c1.x), s_g), S(c0.y)), ddP), s);
+        const F2 rs = rcp(s);  // one reciprocal for both accelerations
+        const F2 q1 = mul(sub(mul(mul(S(c1.x), s_g), S(c0.y)), ddP), rs);
         const F2 aR = add(add(add(S(c0.w), q1), dgR), mul(mul(add(S(2.f * V), wc), wc), S(iR)));
-        const F2 q2 = fdiv(mul(dPdphi, S(-1.f)), mul(s, S(c1.w)));
+        const F2 q2 = mul(mul(dPdphi, S(-1.f)), mul(rs, S(iR)));
         const F2 ap = sub(add(q2, dgp), mul(mul(uc, add(S(V), wc)), S(iR)));
         nu1 = fma(S(dt), aR, uc);
         nw1 = fma(S(dt), ap, wc);
@@ -363,8 +364,9 @@ __device__ __forceinline__ void hydro32p_tile(
       const F2 s2 = fma(mul(S(dt), sub(FF[xf], FF[xf + LF])), S(iv), sgi);
       const F2 sn = add(S(S0), s2);
       const F2 d = make_float2(sn.x < 1e-10f ? 1e-10f : sn.x, sn.y < 1e-10f ? 1e-10f : sn.y);
-      const F2 u2 = fdiv(fma(mul(S(dt), sub(FR[xf], FR[xf + LF])), S(iv), mul(s, u1i)), d);
-      const F2 w2 = fdiv(fma(mul(S(dt), sub(GB[xf], GA[xf + LF])), S(iv), mul(s, w1i)), d);
+      const F2 rd = rcp(d);
+      const F2 u2 = mul(fma(mul(S(dt), sub(FR[xf], FR[xf + LF])), S(iv), mul(s, u1i)), rd);
+      const F2 w2 = mul(fma(mul(S(dt), sub(GB[xf], GA[xf + LF])), S(iv), mul(s, w1i)), rd);
       SG[xs] = s2;
       U2[xs] = u2;
       W2[xs] = w2;
@@ -429,8 +431,9 @@ __device__ __forceinline__ void hydro32p_tile(
         const F2 sn3 = add(S(S0), s3);
         const bool flx = sn3.x < 1e-10f, fly = sn3.y < 1e-10f;
         const F2 d = make_float2(flx ? 1e-10f : sn3.x, fly ? 1e-10f : sn3.y);
-        const F2 u3 = fdiv(fma(mul(S(dt), sub(fr, fr1)), S(iv), mul(sn2, u2)), d);
-        const F2 w3 = fdiv(fma(mul(S(dt), sub(fg, fg1)), S(iv), mul(sn2, w2)), d);
+        const F2 rd = rcp(d);
+        const F2 u3 = mul(fma(mul(S(dt), sub(fr, fr1)), S(iv), mul(sn2, u2)), rd);
+        const F2 w3 = mul(fma(mul(S(dt), sub(fg, fg1)), S(iv), mul(sn2, w2)), rd);
         s3 = make_float2(flx ? 1e-10f - S0 : s3.x, fly ? 1e-10f - S0 : s3.y);
         const size_t q = (size_t)i * Nphi + jc;
         const float R32 = c2.w;
@@ -457,8 +460,9 @@ __device__ __forceinline__ void hydro32p_tile(
         // CFL rate of the new state (hydro.hpp:54-57)
         const F2 scl = make_float2(flx ? 1e-10f : sn3.x, fly ? 1e-10f : sn3.y);
         const float gk = g.gamma * g.Kpoly;
-        const F2 cs = G2 ? make_float2(sqrtf(gk * scl.x), sqrtf(gk * scl.y))
-                         : make_float2(sqrtf(gk * powf(scl.x, g.gamma - 1.f)), sqrtf(gk * powf(scl.y, g.gamma - 1.f)));
+        const F2 cs = G2 ? make_float2(sqrt_pos(gk * scl.x), sqrt_pos(gk * scl.y))
+                         : make_float2(sqrt_pos(gk * powf(scl.x, g.gamma - 1.f)),
+                                       sqrt_pos(gk * powf(scl.y, g.gamma - 1.f)));
         const float V = c0.z, idR = RC(tInvdR, i), idl = c2.y;
         const F2 rate = fma(add(make_float2(fabsf(V + w3.x), fabsf(V + w3.y)), cs), S(idl),
                             mul(add(make_float2(fabsf(u3.x), fabsf(u3.y)), cs), S(idR)));

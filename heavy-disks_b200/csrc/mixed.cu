@@ -1432,6 +1432,8 @@ struct MixedGroup {
   int kind = MixedState::kHydroPacked;
   bool g2 = false;
   int ns[6] = {0, 0, 0, 0, 0, 0};
+  bool persist = true;  // products by the persistent 128 x 128 kernel (DISKGPU_GROUP_GEMM=tile: per-tile kernel)
+  int nsm = 148;
   tc::GemmDisk *gd[4] = {nullptr, nullptr, nullptr, nullptr};  // per product: one entry per disk
   HydroDisk *hd = nullptr;
 };
@@ -1450,8 +1452,15 @@ std::string mixed_group_key(const dg_handle *h) {
 
 template <int MODE, bool A_MN, bool B_MN, bool PER_A>
 static cudaError_t gemm_group(const CUtensorMap &Ch, const CUtensorMap &Cl, const tc::GemmDisk *d, int G, int M,
-                              int N, int K, cudaStream_t st, int ns, bool prepare) {
+                              int N, int K, cudaStream_t st, int ns, bool prepare, bool persist = false,
+                              int nsm = 148) {
   if (M % tc::BM || N % tc::BN || K % tc::BK) return cudaErrorInvalidValue;
+  if (persist && N % tc::BN2 == 0) {
+    auto kp = tc::k_gemm_group_persist<MODE, A_MN, B_MN, PER_A>;
+    if (prepare) return smem_attrs((const void *)kp, tc::kSmemP);
+    const int tn = N / tc::BN2, tm = M / tc::BM, nt = tn * tm * G;
+    return launch_pdl(kp, dim3(nt < nsm ? nt : nsm), dim3(tc::kThreadsP), tc::kSmemP, st, Ch, Cl, d, tn, tm, nt);
+  }
   const int nk = K / tc::BK;
   if (ns == 0) ns = nk <= 1 ? 1 : (nk <= 2 ? 2 : tc::STAGES);
   const int NS = ns <= 1 ? 1 : (ns <= 2 ? 2 : tc::STAGES);
@@ -1477,16 +1486,16 @@ static int group_launch(MixedGroup *g, cudaStream_t st, bool prepare) {
   // G1: X1[c][i] = Fphi[c][:] . Sx[i][:];  G2: Wt[c][p] = KW[c][p] X1[c][:] . Cu[p][:];
   // G3: Z[i][c] = CuT[i][:] . Wt[c][:];    G4: dPhi[i][j] = phiscale[i] Z[i][:] . Gphi[j][:]
   e = gemm_group<tc::kEpiSplit, false, false, false>(X.mFphi[0], X.mFphi[1], g->gd[0], G, Nphi, Nu, Nphi, st, g->ns[0],
-                                                       prepare);
+                                                       prepare, g->persist, g->nsm);
   if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: phi DFT", cudaGetErrorString(e));
   e = gemm_group<tc::kEpiSplitScaled, false, false, true>(X.mCu[0], X.mCu[1], g->gd[1], G, Nphi, 2 * Nu, Nu, st,
-                                                          g->ns[1], prepare);
+                                                          g->ns[1], prepare, g->persist, g->nsm);
   if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: u DFT x khat", cudaGetErrorString(e));
   e = gemm_group<tc::kEpiSplit, false, false, false>(X.mCuT[0], X.mCuT[1], g->gd[2], G, Nu, Nphi, 2 * Nu, st,
-                                                       g->ns[2], prepare);
+                                                       g->ns[2], prepare, g->persist, g->nsm);
   if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: inverse u DFT", cudaGetErrorString(e));
   e = gemm_group<tc::kEpiRowScaleF32, false, false, true>(X.mGphi[0], X.mGphi[1], g->gd[3], G, Nu, Nphi, Nphi, st,
-                                                          g->ns[5], prepare);
+                                                          g->ns[5], prepare, g->persist, g->nsm);
   if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: inverse phi DFT", cudaGetErrorString(e));
   const bool packed = g->kind == MixedState::kHydroPacked;
   auto hk = packed ? (g->g2 ? k_hydro32p_group<true> : k_hydro32p_group<false>)
@@ -1531,6 +1540,13 @@ MixedGroup *mixed_group_create(const std::vector<dg_handle *> &disks, std::strin
   g->kind = XL.hydro_kind;
   g->g2 = XL.rows.gamma2 != 0;
   for (int k = 0; k < 6; ++k) g->ns[k] = XL.ns[k];
+  {
+    const char *gg = getenv("DISKGPU_GROUP_GEMM");
+    g->persist = !(gg && strcmp(gg, "tile") == 0);
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->lead->dev) == cudaSuccess && nsm > 0)
+      g->nsm = nsm;
+  }
   const int G = (int)disks.size(), Nu = XL.Nu, Nphi = XL.Nphi;
   std::vector<tc::GemmDisk> gd[4];
   std::vector<HydroDisk> hd(G);

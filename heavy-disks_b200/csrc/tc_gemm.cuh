@@ -357,6 +357,59 @@ __device__ __forceinline__ void epi_mlp(const GemmArgs &a, int row, int col, con
   }
 }
 
+// The epilogue of one 32-column accumulator chunk of row `row`, columns col..col+31.
+template <int MODE>
+__device__ __forceinline__ void epi_chunk(const GemmArgs &args, int row, int col, const uint32_t (&r)[32], int lane) {
+  if (MODE == kEpiStoreBounded) {
+    epi_mlp_bounded<MODE>(args, row, col, r);
+    return;
+  }
+  if (MODE >= kEpiMlpAct) {
+    epi_mlp<MODE>(args, row, col, r);
+    return;
+  }
+  if (MODE >= kEpiPhiToXin) {
+    epi_factored<MODE>(args, row, col, r, lane);
+    return;
+  }
+  if (MODE == kEpiRowScaleF32) {
+    const float sc = args.row_scale[row];
+    float4 *o = reinterpret_cast<float4 *>(args.out_f32 + (size_t)row * args.ldo + col);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      o[q] = make_float4(__uint_as_float(r[4 * q]) * sc, __uint_as_float(r[4 * q + 1]) * sc,
+                         __uint_as_float(r[4 * q + 2]) * sc, __uint_as_float(r[4 * q + 3]) * sc);
+  } else {
+    float v[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
+    if (MODE == kEpiSplitScaled) {
+      const float4 *tb = reinterpret_cast<const float4 *>(args.table + (size_t)row * args.ldo + col);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        float4 t = tb[q];
+        v[4 * q] *= t.x; v[4 * q + 1] *= t.y; v[4 * q + 2] *= t.z; v[4 * q + 3] *= t.w;
+      }
+    }
+    uint32_t ph[16], pl[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      __nv_bfloat16 h0, l0, h1, l1;
+      split_bf16(v[2 * q], h0, l0);
+      split_bf16(v[2 * q + 1], h1, l1);
+      ph[q] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+      pl[q] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+    }
+    uint4 *oh = reinterpret_cast<uint4 *>(args.out_hi + (size_t)row * args.ldo + col);
+    uint4 *ol = reinterpret_cast<uint4 *>(args.out_lo + (size_t)row * args.ldo + col);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      oh[q] = make_uint4(ph[4 * q], ph[4 * q + 1], ph[4 * q + 2], ph[4 * q + 3]);
+      ol[q] = make_uint4(pl[4 * q], pl[4 * q + 1], pl[4 * q + 2], pl[4 * q + 3]);
+    }
+  }
+}
+
 // The body of one CTA tile (blockIdx.x: N tile, blockIdx.y: M tile) of the split GEMM.
 template <int MODE, bool A_MN, bool B_MN, int NS>
 __device__ __forceinline__ void gemm_tile(const CUtensorMap *pAh, const CUtensorMap *pAl, const CUtensorMap *pBh,
@@ -462,55 +515,7 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap *pAh, const CUtensor
     for (int c0 = 0; c0 < BN; c0 += 32) {
       uint32_t r[32];
       tmem_ld32(tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
-      const int col = n0 + c0;
-      if (MODE == kEpiStoreBounded) {
-        epi_mlp_bounded<MODE>(args, row, col, r);
-        continue;
-      }
-      if (MODE >= kEpiMlpAct) {
-        epi_mlp<MODE>(args, row, col, r);
-        continue;
-      }
-      if (MODE >= kEpiPhiToXin) {
-        epi_factored<MODE>(args, row, col, r, lane);
-        continue;
-      }
-      if (MODE == kEpiRowScaleF32) {
-        const float sc = args.row_scale[row];
-        float4 *o = reinterpret_cast<float4 *>(args.out_f32 + (size_t)row * args.ldo + col);
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-          o[q] = make_float4(__uint_as_float(r[4 * q]) * sc, __uint_as_float(r[4 * q + 1]) * sc,
-                             __uint_as_float(r[4 * q + 2]) * sc, __uint_as_float(r[4 * q + 3]) * sc);
-      } else {
-        float v[32];
-#pragma unroll
-        for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
-        if (MODE == kEpiSplitScaled) {
-          const float4 *tb = reinterpret_cast<const float4 *>(args.table + (size_t)row * args.ldo + col);
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            float4 t = tb[q];
-            v[4 * q] *= t.x; v[4 * q + 1] *= t.y; v[4 * q + 2] *= t.z; v[4 * q + 3] *= t.w;
-          }
-        }
-        uint32_t ph[16], pl[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          __nv_bfloat16 h0, l0, h1, l1;
-          split_bf16(v[2 * q], h0, l0);
-          split_bf16(v[2 * q + 1], h1, l1);
-          ph[q] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-          pl[q] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
-        }
-        uint4 *oh = reinterpret_cast<uint4 *>(args.out_hi + (size_t)row * args.ldo + col);
-        uint4 *ol = reinterpret_cast<uint4 *>(args.out_lo + (size_t)row * args.ldo + col);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          oh[q] = make_uint4(ph[4 * q], ph[4 * q + 1], ph[4 * q + 2], ph[4 * q + 3]);
-          ol[q] = make_uint4(pl[4 * q], pl[4 * q + 1], pl[4 * q + 2], pl[4 * q + 3]);
-        }
-      }
+      epi_chunk<MODE>(args, row, n0 + c0, r, lane);
     }
   }
   tc_fence_before();
@@ -544,6 +549,192 @@ __global__ void __launch_bounds__(kThreads, (NS == 1 ? 4 : (NS == 2 ? 2 : 1)))
     gemm_tile<MODE, A_MN, B_MN, NS>(&d.hi, &d.lo, &tmCh, &tmCl, d.args);
   else
     gemm_tile<MODE, A_MN, B_MN, NS>(&tmCh, &tmCl, &d.hi, &d.lo, d.args);
+}
+
+// ---------------------------------------------------------------------------------
+// Persistent form of the group product (batched sweeps).  One CTA per SM walks the tiles
+// of every disk of the group (tile t = blockIdx.x + k gridDim.x; disk, M tile, N tile
+// from t) with its warps specialised: warp 0 drives TMA through an NS2-deep ring of stages
+// that runs ahead across tile boundaries, warp 1 issues the MMAs, warps 2..5 drain TMEM
+// and run the epilogue.  Two TMEM accumulators (128 columns each) let the epilogue of one
+// tile overlap the MMAs of the next.  Tiles are 128 x 128: per byte loaded from L2 twice
+// the MMA work of the 128 x 64 tiles above.  Each output element sees the same sequence
+// of K steps and products as in k_gemm_split.  All waits are bounded as above; on a
+// timeout every role stops at its next wait, in-flight copies are drained, and TMEM is
+// freed.
+constexpr int BN2 = 128;
+constexpr int NS2 = 3;
+constexpr uint32_t kTileB2 = BN2 * BK * 2;
+constexpr uint32_t kStageBytes2 = 2 * kTileA + 2 * kTileB2;  // 64 KB
+constexpr int kThreadsP = 192;
+constexpr uint32_t kTmemColsP = 2 * BN2;
+constexpr size_t kSmemP = (size_t)NS2 * kStageBytes2 + 1024;
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <int MODE, bool A_MN, bool B_MN, bool PER_A>
+__global__ void __launch_bounds__(kThreadsP, 1)
+    k_gemm_group_persist(const __grid_constant__ CUtensorMap tmCh, const __grid_constant__ CUtensorMap tmCl,
+                         const GemmDisk *__restrict__ disks, int tiles_n, int tiles_m, int ntiles) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  __shared__ __align__(8) uint64_t full_bar[NS2], empty_bar[NS2], acc_full[2], acc_empty[2];
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < NS2; ++q) {
+      mbar_init(&full_bar[q], 1);
+      mbar_init(&empty_bar[q], 1);
+    }
+    for (int q = 0; q < 2; ++q) {
+      mbar_init(&acc_full[q], 1);
+      mbar_init(&acc_empty[q], 4);  // one arrival per epilogue warp
+    }
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tmem_alloc(&tmem_slot, kTmemColsP);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  pdl_wait();  // operands come from the previous kernel on the stream
+  pdl_trigger();
+  const int per_disk = tiles_n * tiles_m;
+  auto decode = [&](int t, int &z, int &m0, int &n0) {
+    z = t / per_disk;
+    const int r = t - z * per_disk;
+    m0 = (r / tiles_n) * BM;
+    n0 = (r - (r / tiles_n) * tiles_n) * BN2;
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- TMA producer ----
+      uint32_t it = 0;
+      int *st_word = nullptr;
+      for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x) {
+        int z, m0, n0;
+        decode(t, z, m0, n0);
+        const GemmDisk &d = disks[z];
+        st_word = d.args.status;
+        const CUtensorMap *Ah = PER_A ? &d.hi : &tmCh, *Al = PER_A ? &d.lo : &tmCl;
+        const CUtensorMap *Bh = PER_A ? &tmCh : &d.hi, *Bl = PER_A ? &tmCl : &d.lo;
+        const int nk = d.args.K / BK;
+        for (int kc = 0; kc < nk; ++kc) {
+          const uint32_t sidx = it % NS2;
+          if (it >= NS2 && !mbar_wait(&empty_bar[sidx], ((it / NS2) - 1) & 1, st_word)) {
+            abort_flag = 1;
+            break;
+          }
+          if (abort_flag) break;
+          uint8_t *st = smem + sidx * kStageBytes2;
+          mbar_arrive_expect_tx(&full_bar[sidx], kStageBytes2);
+          if (A_MN) {
+            tma_load_2d(st, Ah, &full_bar[sidx], m0, kc * BK);
+            tma_load_2d(st + kTileA / 2, Ah, &full_bar[sidx], m0 + 64, kc * BK);
+            tma_load_2d(st + kTileA, Al, &full_bar[sidx], m0, kc * BK);
+            tma_load_2d(st + kTileA + kTileA / 2, Al, &full_bar[sidx], m0 + 64, kc * BK);
+          } else {
+            tma_load_2d(st, Ah, &full_bar[sidx], kc * BK, m0);
+            tma_load_2d(st + kTileA, Al, &full_bar[sidx], kc * BK, m0);
+          }
+          uint8_t *sb = st + 2 * kTileA;
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {  // two 64-wide N chunks (MN-major) or 64-row boxes (K-major)
+            if (B_MN) {
+              tma_load_2d(sb + c * (kTileB2 / 2), Bh, &full_bar[sidx], n0 + 64 * c, kc * BK);
+              tma_load_2d(sb + kTileB2 + c * (kTileB2 / 2), Bl, &full_bar[sidx], n0 + 64 * c, kc * BK);
+            } else {
+              tma_load_2d(sb + c * (kTileB2 / 2), Bh, &full_bar[sidx], kc * BK, n0 + 64 * c);
+              tma_load_2d(sb + kTileB2 + c * (kTileB2 / 2), Bl, &full_bar[sidx], kc * BK, n0 + 64 * c);
+            }
+          }
+          ++it;
+        }
+      }
+      // every issued copy must land before the CTA may exit
+      for (uint32_t j = it > NS2 ? it - NS2 : 0; j < it; ++j) mbar_wait(&full_bar[j % NS2], (j / NS2) & 1, st_word);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer ----
+      const uint32_t idesc = idesc_bf16(BM, BN2, A_MN, B_MN);
+      uint32_t it = 0;
+      int lt = 0;
+      for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++lt) {
+        int z, m0, n0;
+        decode(t, z, m0, n0);
+        const GemmDisk &d = disks[z];
+        const int nk = d.args.K / BK;
+        const int buf = lt & 1;
+        if (lt >= 2 && !mbar_wait(&acc_empty[buf], ((lt >> 1) - 1) & 1, d.args.status)) {
+          abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t acc = tmem + (uint32_t)(buf * BN2);
+        bool ok = true;
+        for (int kc = 0; kc < nk; ++kc, ++it) {
+          const uint32_t sidx = it % NS2;
+          if (!mbar_wait(&full_bar[sidx], (it / NS2) & 1, d.args.status)) {
+            abort_flag = 1;
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          uint8_t *st = smem + sidx * kStageBytes2;
+          const uint64_t dAh = A_MN ? sdesc_mn_sw128(st, kTileA / 2) : sdesc_sw128(st);
+          const uint64_t dAl = A_MN ? sdesc_mn_sw128(st + kTileA, kTileA / 2) : sdesc_sw128(st + kTileA);
+          const uint64_t dBh = B_MN ? sdesc_mn_sw128(st + 2 * kTileA, kTileB2 / 2) : sdesc_sw128(st + 2 * kTileA);
+          const uint64_t dBl =
+              B_MN ? sdesc_mn_sw128(st + 2 * kTileA + kTileB2, kTileB2 / 2) : sdesc_sw128(st + 2 * kTileA + kTileB2);
+          const uint64_t stepA = A_MN ? (2048 >> 4) : (32 >> 4), stepB = B_MN ? (2048 >> 4) : (32 >> 4);
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+            const uint64_t oa = (uint64_t)kk * stepA, ob = (uint64_t)kk * stepB;
+            mma_bf16(acc, dAh + oa, dBh + ob, idesc, (kc | kk) != 0);
+            mma_bf16(acc, dAh + oa, dBl + ob, idesc, 1u);
+            mma_bf16(acc, dAl + oa, dBh + ob, idesc, 1u);
+          }
+          mma_commit(&empty_bar[sidx]);
+        }
+        if (!ok) break;
+        mma_commit(&acc_full[buf]);  // arrives once this tile's MMAs have completed
+      }
+    }
+  } else {
+    // ---- epilogue: warp w drains TMEM lanes 32 (w % 4) .. + 31 ----
+    const int qd = warp & 3;
+    int lt = 0;
+    for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++lt) {
+      int z, m0, n0;
+      decode(t, z, m0, n0);
+      const GemmDisk &d = disks[z];
+      const int buf = lt & 1;
+      if (!mbar_wait(&acc_full[buf], (lt >> 1) & 1, d.args.status)) {
+        abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const int row = m0 + qd * 32 + lane;
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN2; c0 += 32) {
+        uint32_t r[32];
+        tmem_ld32(tmem + (uint32_t)(buf * BN2) + ((uint32_t)(qd * 32) << 16) + (uint32_t)c0, r);
+        epi_chunk<MODE>(d.args, row, n0 + c0, r, lane);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[buf]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kTmemColsP);
 }
 
 }  // namespace tc

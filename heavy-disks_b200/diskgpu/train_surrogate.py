@@ -3,10 +3,11 @@
   python -m diskgpu.train_surrogate --runs 512 --grid 128 --tlim 16 --out <dir>
 
 Draws sweep points with the sweep law (diskgpu.sweep.draw, fixed seed), runs them in
-batches of disks advanced together (dg_batch, mixed precision), fits gamma / Omega_p /
-saturated |C2|/|C0| from each disk's mode records, trains the MLP on 95 % and reports its
-error on the 5 % held out against the hydro's own values.  Writes dataset.npz,
-surrogate.npz (network, standardisation and report) and report.json to --out.
+batches of disks advanced together (dg_batch, mixed precision; same-grid disks step as one
+group), fits gamma / Omega_p / saturated |C2|/|C0| from each disk's mode records, trains
+the MLP on 95 % and reports its error on the 5 % held out against the hydro's own values.
+Writes sweep_<grid>_dataset.npz, surrogate.npz (network, standardisation and report) and
+report.json to --out.
 """
 from __future__ import annotations
 
@@ -45,7 +46,7 @@ def run_points(pts, tlim, batch=128, dtout=0.25):
             params.append((p, q))
         with Batch([p for p, _ in params]) as b:
             b.init_standard()
-            recs, t, steps = b.advance(tlim, dtout=dtout)
+            recs, t, steps = b.advance(tlim, dtout=dtout, steps_per_launch=64)
         for pt, (p, q), rec, st in zip(chunk, params, recs, steps):
             g, w, sr = fit_record(rec)
             rows.append([pt.Qmin, pt.mass_ratio, pt.soft_over_r, pt.gamma, q, g, w, sr, st])
@@ -67,7 +68,7 @@ def main():
     t0 = time.time()
     data = run_points(pts, a.tlim, batch=a.batch)
     t_hydro = time.time() - t0
-    np.savez(os.path.join(a.out, "dataset.npz"), data=data,
+    np.savez(os.path.join(a.out, f"sweep_{a.grid}_dataset.npz"), data=data,
              columns=np.array(["Qmin", "mass_ratio", "soft_over_r", "gamma_eos", "Qmin_achieved", "gamma",
                                "omega_p", "sat_ratio", "steps"]))
     X, Y = data[:, :4], data[:, 5:8]
