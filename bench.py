@@ -265,6 +265,12 @@ def gravity_parts(precision, Nu, Nphi):
         g4 = (Nu // 4) * (6 * 128 * 64 * 64 + 6 * 128 * 32 * 64)
         g4name = ("fused inverse phi transform (k_phiinv: complex 32-point + real-output 32-point tcgen05 "
                   "stages, potential scaling)")
+    if Nphi == 4096 and Nu % 1024 == 0 and Nu != 1024:  # four-step 64 x 64 phi transforms, two products each
+        g1 = 6 * 128 * (Nu * 64) * 64 + 6 * (64 * Nu) * 128 * 128
+        g1name = "four-step phi transform (two k_gemm_split passes: real 64-point over j1, twiddle, complex 64-point)"
+        g4 = 6 * (64 * Nu) * 128 * 128 + 6 * (64 * Nu) * 64 * 128
+        g4name = ("four-step inverse phi transform (two k_gemm_split passes: complex 64-point, twiddle, real-output "
+                  "64-point, potential scaling)")
     if Nu % 1024 == 0:
         A, nm = Nu // 32, ((Nphi // 2 + 1) + 3) // 4 * 4
         u = 6 * 128 * (nm * A) * 64 + 2 * 6 * (nm * 64) * (2 * A) * (2 * A) + 6 * (nm * A) * 64 * 128

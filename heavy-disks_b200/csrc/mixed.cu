@@ -102,6 +102,12 @@ struct MixedState {
   float2 *twp = nullptr; // W_M^{p2 i1} with padded rows, [64][kUcTwLd]
   CUtensorMap mXin[2], mTb[2], mYk[2], mUb[2], mRB[2], mRA[2], mRGA[2], mRGB[2], mZmn[2];
   bool tables_ready = false;
+  // Nphi = 4096 on grids whose u convolution runs as four passes: both phi transforms in
+  // two split-BF16 passes each (64 x 64, four-step) instead of the dense DFT products
+  bool phi4096 = false;
+  SplitBuf PhA1, PhB2f, PhB1i, PhB2i, PhT, PhX, PhV;
+  float2 *twph = nullptr;  // W_4096^{m1 j2}, [64][64]
+  CUtensorMap mSxBlk[2], mPhA1[2], mPhB2f[2], mPhB1i[2], mPhB2i[2], mPhT[2], mPhX[2], mPhV[2];
   // Failure-detection test: DISKGPU_TEST_ROWTILE_STALL=<row tile> at handle creation makes
   // the first self-gravity step enqueued outside a graph capture raise that tile row's
   // counter once more after its hydro has finished, so the next phi transform's bounded
@@ -267,6 +273,27 @@ __global__ void k_tab_kw(float *KW, const double2 *khat, int Nu, int Nphi) {
     int pp = p > Nu ? p - Nu : p;
     double wgt = (p == 0 || p == Nu) ? 1.0 : 2.0;
     KW[k] = (float)(wgt / M * khat[(size_t)m * M + pp].x);
+  }
+}
+
+// Tables of the four-step phi transforms at Nphi = 4096 (m = m1 + 64 m2, j = 64 j1 + j2):
+// PhA1[(m1, ri)][j1] = cos / -sin (2 pi m1 j1 / 64), the real-input 64-point DFT over j1;
+// PhB2i[j1][(m1, ri)] = cos / -sin (2 pi j1 m1 / 64) / N, the real part of the inverse
+// 64-point DFT over m1 with the inverse transform's 1 / N.
+__global__ void k_tab_ph4096(SplitBuf A1, SplitBuf B2i, int N) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 128 * 64; q += gridDim.x * blockDim.x) {
+    {
+      const int row = q / 64, j1 = q % 64, m1 = row >> 1, ri = row & 1;
+      double sn, cs;
+      sincospi(2.0 * (double)((m1 * j1) % 64) / 64.0, &sn, &cs);
+      put_split(A1, q, ri ? -sn : cs);
+    }
+    {
+      const int j1 = q / 128, col = q % 128, m1 = col >> 1, ri = col & 1;
+      double sn, cs;
+      sincospi(2.0 * (double)((j1 * m1) % 64) / 64.0, &sn, &cs);
+      put_split(B2i, q, (ri ? -sn : cs) / N);
+    }
   }
 }
 
@@ -710,6 +737,39 @@ int dg_handle::mixed_init() {
                make_map(&X.mRGB[0], X.RGB.hi, 64, 128, tc::BN) && make_map(&X.mRGB[1], X.RGB.lo, 64, 128, tc::BN) &&
                make_map(&X.mZmn[0], X.Z.hi, Nphi, Nu, 64) && make_map(&X.mZmn[1], X.Z.lo, Nphi, Nu, 64);
     if (!okf) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed (factored path)");
+    X.phi4096 = !X.fused_u && Nphi == 4096;
+    if (X.phi4096) {
+      const size_t big = (size_t)64 * Nu * 128;  // T, X, V: [64 Nu][128]
+      XK(alloc_split(X.PhA1, (size_t)128 * 64)); XK(alloc_split(X.PhB2i, (size_t)64 * 128));
+      XK(alloc_split(X.PhB2f, (size_t)128 * 128)); XK(alloc_split(X.PhB1i, (size_t)128 * 128));
+      XK(alloc_split(X.PhT, big)); XK(alloc_split(X.PhX, big)); XK(alloc_split(X.PhV, big));
+      XK(dalloc(&X.twph, (size_t)64 * 64));
+      k_tab_ph4096<<<32, 256, 0, st>>>(X.PhA1, X.PhB2i, Nphi);
+      k_tab_cblock<<<64, 256, 0, st>>>(X.PhB2f, 64, 64, 64, -1);  // W_64^{m2 j2}
+      k_tab_cblock<<<64, 256, 0, st>>>(X.PhB1i, 64, 64, 64, +1);  // W_64^{-j2 m2}
+      k_tab_tw<<<64, 256, 0, st>>>(X.twph, 64, 64);                // W_4096^{m1 j2}
+      XK(cudaGetLastError());
+      bool ok4 = make_map(&X.mSxBlk[0], X.Sx.hi, (uint64_t)Nu * 64, 64, 64) &&
+                 make_map(&X.mSxBlk[1], X.Sx.lo, (uint64_t)Nu * 64, 64, 64) &&
+                 make_map(&X.mPhA1[0], X.PhA1.hi, 128, 64, tc::BM) && make_map(&X.mPhA1[1], X.PhA1.lo, 128, 64, tc::BM) &&
+                 make_map(&X.mPhB2f[0], X.PhB2f.hi, 128, 128, tc::BN) &&
+                 make_map(&X.mPhB2f[1], X.PhB2f.lo, 128, 128, tc::BN) &&
+                 make_map(&X.mPhB1i[0], X.PhB1i.hi, 128, 128, tc::BN) &&
+                 make_map(&X.mPhB1i[1], X.PhB1i.lo, 128, 128, tc::BN) &&
+                 make_map(&X.mPhB2i[0], X.PhB2i.hi, 64, 128, tc::BN) && make_map(&X.mPhB2i[1], X.PhB2i.lo, 64, 128, tc::BN) &&
+                 make_map(&X.mPhT[0], X.PhT.hi, (uint64_t)64 * Nu, 128, tc::BM) &&
+                 make_map(&X.mPhT[1], X.PhT.lo, (uint64_t)64 * Nu, 128, tc::BM) &&
+                 make_map(&X.mPhX[0], X.PhX.hi, (uint64_t)64 * Nu, 128, tc::BM) &&
+                 make_map(&X.mPhX[1], X.PhX.lo, (uint64_t)64 * Nu, 128, tc::BM) &&
+                 make_map(&X.mPhV[0], X.PhV.hi, (uint64_t)64 * Nu, 128, tc::BM) &&
+                 make_map(&X.mPhV[1], X.PhV.lo, (uint64_t)64 * Nu, 128, tc::BM);
+      if (!ok4) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed (phi transforms at 4096)");
+      XK((prepare_gemm<tc::kEpiPhiS1, false, true>()));
+      XK((prepare_gemm<tc::kEpiPhiS2, false, false>()));
+      XK((prepare_gemm<tc::kEpiI2ToX, false, false>()));
+      XK((prepare_gemm<tc::kEpiPhiQ1, false, false>()));
+      XK((prepare_gemm<tc::kEpiPhiQ2, false, false>()));
+    }
     XK((prepare_gemm<tc::kEpiPhiToXin, false, false>()));
     XK((prepare_gemm<tc::kEpiTwiddleF1, false, true>()));
     XK((prepare_gemm<tc::kEpiSplitScaled, true, false>()));
@@ -767,9 +827,10 @@ void dg_handle::mixed_release() {
   }
   SplitBuf *bufs[] = {&X.Sx, &X.X1, &X.Wt, &X.Z, &X.Fphi, &X.Cu, &X.CuT, &X.Gphi,
                       &X.Xin, &X.Tb, &X.Yk, &X.Ub, &X.RB, &X.RA, &X.RGA, &X.RGB, &X.PA, &X.PB,
-                      &X.IA, &X.IB, &X.Zt};
+                      &X.IA, &X.IB, &X.Zt, &X.PhA1, &X.PhB2f, &X.PhB1i, &X.PhB2i, &X.PhT, &X.PhX, &X.PhV};
   for (SplitBuf *b : bufs) free_split(*b);
-  void *ptrs[] = {X.KW, X.dPhi, X.rowpend, X.phiscale, X.rowbuf, X.rowtab, X.rowbufd, X.KW2, X.tw, X.khm, X.twp, X.twphi};
+  void *ptrs[] = {X.KW,  X.dPhi, X.rowpend, X.phiscale, X.rowbuf, X.rowtab, X.rowbufd,
+                  X.KW2, X.tw,   X.khm,     X.twp,      X.twphi,  X.twph};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   delete mx;
@@ -1216,6 +1277,15 @@ int dg_handle::mixed_gravity() {
                        X.rs_wait ? X.rowpend : nullptr};
       XK(launch_pdl(tc::k_phifwd, dim3(Nu / tc::kPfRows), dim3(tc::kPfThreads), tc::kPfSmem, st, X.mPA[0], X.mPA[1],
                     X.mPB[0], X.mPB[1], f));
+    } else if (X.phi4096) {
+      // S1: real 64-point DFT over j1 (s read as [(i, j1)][j2]), x W_N^{j2 m1} -> T[(m1, i)][(j2, ri)]
+      a.out_hi = X.PhT.hi; a.out_lo = X.PhT.lo; a.twiddle = X.twph;
+      XK((gemm<tc::kEpiPhiS1, false, true>(X.mPhA1[0], X.mPhA1[1], X.mSxBlk[0], X.mSxBlk[1], 128, Nu * 64, 64, a,
+                                             st, 0)));
+      // S2: complex 64-point DFT over j2 -> modes m = m1 + 64 m2 <= N/2 into Xin
+      a.out_hi = X.Xin.hi; a.out_lo = X.Xin.lo;
+      XK(gemm<tc::kEpiPhiS2>(X.mPhT[0], X.mPhT[1], X.mPhB2f[0], X.mPhB2f[1], 64 * Nu, 128, 128, a, st, 0));
+      a.twiddle = X.tw;
     } else {
       XK(gemm<tc::kEpiPhiToXin>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st, X.ns[0]));
     }
@@ -1239,9 +1309,15 @@ int dg_handle::mixed_gravity() {
       // I1: inverse A-point DFT over p1, conjugate twiddle -> Ub[(m, i1)][(p2, ri)]
       a.out_hi = X.Ub.hi; a.out_lo = X.Ub.lo; a.table = nullptr;
       XK(gemm<tc::kEpiTwiddleI1>(X.mYk[0], X.mYk[1], X.mRGA[0], X.mRGA[1], nm * 64, 2 * A, 2 * A, a, st, X.ns[3]));
-      // I2: inverse 64-point DFT over p2 (the 32 physical i2) -> Z[c][i]
-      a.out_hi = X.Z.hi; a.out_lo = X.Z.lo;
-      XK(gemm<tc::kEpiI2ToZ>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st, X.ns[4]));
+      // I2: inverse 64-point DFT over p2 (the 32 physical i2) -> Z[c][i], or at Nphi = 4096
+      // the full Hermitian spectrum X[(m % 64, i)][(m / 64, ri)] of the four-step inverse
+      if (X.phi4096) {
+        a.out_hi = X.PhX.hi; a.out_lo = X.PhX.lo;
+        XK(gemm<tc::kEpiI2ToX>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st, X.ns[4]));
+      } else {
+        a.out_hi = X.Z.hi; a.out_lo = X.Z.lo;
+        XK(gemm<tc::kEpiI2ToZ>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st, X.ns[4]));
+      }
     }
     XK(prof_end(DG_PROF_GRAV_U));
     // G4: inverse phi DFT: the fused two-stage kernel from Zt, or a product with Z as an
@@ -1252,7 +1328,14 @@ int dg_handle::mixed_gravity() {
     const int rp_val =
         X.hydro_kind == MixedState::kHydroPacked ? (Nphi + kTileJp - 1) / kTileJp : (Nphi + kTileJ - 1) / kTileJ;
     XK(prof_begin(DG_PROF_GRAV_PHI_INV));
-    if (X.fused_phi) {
+    if (X.phi4096) {
+      // Q1: inverse 64-point DFT over m2, x W_N^{-j2 m1} -> V[(i, j2)][(m1, ri)]
+      a.out_hi = X.PhV.hi; a.out_lo = X.PhV.lo; a.twiddle = X.twph;
+      XK(gemm<tc::kEpiPhiQ1>(X.mPhX[0], X.mPhX[1], X.mPhB1i[0], X.mPhB1i[1], 64 * Nu, 128, 128, a, st, 0));
+      // Q2: real part of the inverse 64-point DFT over m1, / N, x (-G du dphi / sqrt(R))
+      a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.row_scale = X.phiscale;
+      XK(gemm<tc::kEpiPhiQ2>(X.mPhV[0], X.mPhV[1], X.mPhB2i[0], X.mPhB2i[1], 64 * Nu, 64, 128, a, st, 0));
+    } else if (X.fused_phi) {
       tc::PhiInvArgs f{X.Zt.hi, X.Zt.lo, X.twphi, X.phiscale, X.dPhi, Nphi, &ctl->status, rp, rp_n, rp_val};
       XK(launch_pdl(tc::k_phiinv, dim3(Nu / tc::kPiRows), dim3(tc::kPiThreads), tc::kPiSmem, st, X.mIA[0], X.mIA[1],
                     X.mIB[0], X.mIB[1], f));
@@ -1299,6 +1382,7 @@ int dg_handle::mixed_hydro_kernels() const {
 
 int dg_handle::mixed_gravity_kernels() const {
   if (!u_factored(p.Nu)) return 4;
+  if (mx && mx->phi4096) return 8;
   return u_fused(p.Nu) ? 3 : 6;
 }
 

@@ -48,6 +48,14 @@ enum EpiMode : int {
   kEpiMlpOut = 8,       // D + bias[col] -> out_f32 (linear head)
   kEpiMlpBack = 9,      // d = D * SiLU'(table[row][col]) -> out_f32 and split(d) -> out_hi / out_lo
   kEpiStoreBounded = 10,  // D -> out_f32[row][col] for row < lim_m, col < lim_n (weight gradients)
+  // factored phi transforms at Nphi = 4096 = 64 x 64 (j = 64 j1 + j2, m = m1 + 64 m2;
+  // mixed.cu documents the passes).  The S1 product reads its B operand (the gravity
+  // operand s[i][64 j1 + j2] as the [(i, j1)][j2] matrix) in 64 x 64 blocks per row i.
+  kEpiPhiS1 = 11,       // rows (m1, ri), cols (i, j2): x W_N^{j2 m1} -> T[(m1, i)][(j2, ri)]
+  kEpiPhiS2 = 12,       // rows (m1, i), cols (m2, ri): modes m <= N/2 -> Xin[(i2, ri)][(m, i1)]
+  kEpiI2ToX = 13,       // rows (m, i1), cols (i2, ri): X and its conjugate -> X[(m % 64, i)][(m / 64, ri)]
+  kEpiPhiQ1 = 14,       // rows (m1, i), cols (j2, ri): x W_N^{-j2 m1} -> V[(i, j2)][(m1, ri)]
+  kEpiPhiQ2 = 15,       // rows (i, j2), cols j1: x row_scale[i] -> out_f32[i][64 j1 + j2]
 };
 
 struct GemmArgs {
@@ -357,11 +365,99 @@ __device__ __forceinline__ void epi_mlp(const GemmArgs &a, int row, int col, con
   }
 }
 
+// Epilogues of the factored phi transforms at Nphi = 4096 (twiddle: W_N^{m1 j2} as
+// [64][64], A = Nu / 32, nmodes = padded complex-mode count of the u stage).
+template <int MODE>
+__device__ __forceinline__ void epi_phi4096(const GemmArgs &a, int row, int col, const uint32_t (&r)[32], int lane) {
+  const int A = a.fa, Nu = 32 * A, N = a.nphi, half = N / 2;
+  auto put = [&](size_t k, float x) {
+    __nv_bfloat16 h, l;
+    split_bf16(x, h, l);
+    a.out_hi[k] = h;
+    a.out_lo[k] = l;
+  };
+  auto put2 = [&](size_t k, float x, float y) {  // (x, y) at k, k + 1 (k even): one word per plane
+    __nv_bfloat16 h0, l0, h1, l1;
+    split_bf16(x, h0, l0);
+    split_bf16(y, h1, l1);
+    *reinterpret_cast<uint32_t *>(a.out_hi + k) =
+        (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+    *reinterpret_cast<uint32_t *>(a.out_lo + k) =
+        (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+  };
+  if (MODE == kEpiPhiS1) {
+    // rows (m1, ri): re / im of one m1 in lanes l, l^1; cols (i, j2), the chunk inside one i
+    const int m1 = row >> 1, ri = row & 1;
+    const int i = col >> 6, j2b = col & 63;
+    const size_t base = ((size_t)m1 * Nu + i) * 128 + ri;
+    const float2 *tw = a.twiddle + m1 * 64 + j2b;
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+      const float v = __uint_as_float(r[q]);
+      const float o = __shfl_xor_sync(0xffffffffu, v, 1);
+      const float re = ri ? o : v, im = ri ? v : o;
+      const float2 w = __ldg(tw + q);
+      put(base + 2 * (j2b + q), ri ? (re * w.y + im * w.x) : (re * w.x - im * w.y));
+    }
+  } else if (MODE == kEpiPhiS2) {
+    // rows (m1, i), cols (m2, ri) pairs in-thread -> the u stage's operand Xin
+    const int m1 = row / Nu, i = row - m1 * Nu;
+    const int i2 = i / A, i1 = i - i2 * A;
+    const size_t ld = (size_t)a.nmodes * A;
+#pragma unroll
+    for (int q = 0; q < 32; q += 2) {
+      const int m = m1 + 64 * ((col + q) >> 1);
+      if (m > half) continue;
+      put((size_t)(2 * i2) * ld + (size_t)m * A + i1, __uint_as_float(r[q]));
+      if (m != 0 && m != half) put((size_t)(2 * i2 + 1) * ld + (size_t)m * A + i1, __uint_as_float(r[q + 1]));
+    }
+  } else if (MODE == kEpiI2ToX) {
+    // rows (m, i1), cols (i2, ri) pairs in-thread -> the full Hermitian spectrum X
+    const int m = row / A, i1 = row - m * A;
+    if (m > half) return;  // padding modes
+    const int i2b = col >> 1;
+#pragma unroll
+    for (int q = 0; q < 32; q += 2) {
+      const size_t i = (size_t)i1 + (size_t)A * (i2b + (q >> 1));
+      const float re = __uint_as_float(r[q]);
+      const float im = (m == 0 || m == half) ? 0.f : __uint_as_float(r[q + 1]);
+      put2(((size_t)(m & 63) * Nu + i) * 128 + 2 * (m >> 6), re, im);
+      if (m != 0 && m != half) {
+        const int mc = N - m;
+        put2(((size_t)(mc & 63) * Nu + i) * 128 + 2 * (mc >> 6), re, -im);
+      }
+    }
+  } else if (MODE == kEpiPhiQ1) {
+    // rows (m1, i), cols (j2, ri) pairs in-thread: x conj(W_N^{m1 j2}) -> V[(i, j2)][(m1, ri)]
+    const int m1 = row / Nu, i = row - m1 * Nu;
+    const int j2b = col >> 1;
+    const float2 *tw = a.twiddle + m1 * 64 + j2b;
+#pragma unroll
+    for (int q = 0; q < 32; q += 2) {
+      const float re = __uint_as_float(r[q]), im = __uint_as_float(r[q + 1]);
+      const float2 w = __ldg(tw + (q >> 1));
+      put2(((size_t)i * 64 + j2b + (q >> 1)) * 128 + 2 * m1, re * w.x + im * w.y, im * w.x - re * w.y);
+    }
+  } else if (MODE == kEpiPhiQ2) {
+    // rows (i, j2), cols j1: dPhi[i][64 j1 + j2] (lanes: consecutive j2, so coalesced)
+    const int i = row >> 6, j2 = row & 63;
+    const float sc = a.row_scale[i];
+    float *o = a.out_f32 + (size_t)i * N + j2;
+#pragma unroll
+    for (int q = 0; q < 32; ++q) o[64 * (col + q)] = __uint_as_float(r[q]) * sc;
+  }
+  (void)lane;
+}
+
 // The epilogue of one 32-column accumulator chunk of row `row`, columns col..col+31.
 template <int MODE>
 __device__ __forceinline__ void epi_chunk(const GemmArgs &args, int row, int col, const uint32_t (&r)[32], int lane) {
   if (MODE == kEpiStoreBounded) {
     epi_mlp_bounded<MODE>(args, row, col, r);
+    return;
+  }
+  if (MODE >= kEpiPhiS1) {
+    epi_phi4096<MODE>(args, row, col, r, lane);
     return;
   }
   if (MODE >= kEpiMlpAct) {
@@ -464,7 +560,10 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap *pAh, const CUtensor
         tma_load_2d(st, pAh, &full_bar[s], kc * BK, m0);
         tma_load_2d(st + kTileA, pAl, &full_bar[s], kc * BK, m0);
       }
-      if (B_MN) {  // [K][N] in global: one 64-wide N chunk
+      if (B_MN && MODE == kEpiPhiS1) {  // the [(i, j1)][j2] view of s: N chunk n0 = row i's 64 columns
+        tma_load_2d(st + 2 * kTileA, pBh, &full_bar[s], 0, n0 + kc * BK);
+        tma_load_2d(st + 2 * kTileA + kTileB, pBl, &full_bar[s], 0, n0 + kc * BK);
+      } else if (B_MN) {  // [K][N] in global: one 64-wide N chunk
         tma_load_2d(st + 2 * kTileA, pBh, &full_bar[s], n0, kc * BK);
         tma_load_2d(st + 2 * kTileA + kTileB, pBl, &full_bar[s], n0, kc * BK);
       } else {

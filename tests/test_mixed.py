@@ -6,6 +6,8 @@ term, so the gravity of a field agrees with the FP64 potential to <= 2e-4 relati
 perturbation fields after 100 steps agree to <= 2e-3 of the perturbation's own size;
 gamma and Omega_p from the same run agree to <= 0.5 % (the mixed path's accuracy
 requirement)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -27,12 +29,13 @@ def _field(Nu, Nphi, seed=0):
 
 
 @pytest.mark.parametrize("Nu,Nphi", [(128, 128), (256, 256), (128, 384), (512, 256), (1024, 256), (1024, 1024),
-                                     (2048, 128), (4096, 128), (128, 2048), (128, 4096)])
+                                     (2048, 128), (4096, 128), (128, 2048), (128, 4096), (2048, 4096)])
 def test_tensor_core_potential_vs_fp64(Nu, Nphi):
     """The split-BF16 DFT convolution against the FP64 FFT potential (<= 2e-4 rel).  The
     grids reach every form: dense u and phi products (128..512), the fused transforms
-    (1024^2), the four-pass factored u convolution with A = 64 and 128 (Nu = 2048, 4096)
-    and the dense phi products at K = 2048 and 4096."""
+    (1024^2), the four-pass factored u convolution with A = 64 and 128 (Nu = 2048, 4096),
+    the dense phi products at K = 2048 and 4096, and the four-step 64 x 64 phi transforms
+    (Nphi = 4096 beside a four-pass u convolution)."""
     Sig = _field(Nu, Nphi)
     ref = O.Kalnajs(Nu, Nphi, eps=0.01).potential(Sig)
     with D.Disk(Nu, Nphi, eps=0.01, precision="mixed") as d:
@@ -60,12 +63,13 @@ def test_state_roundtrip_mixed():
         assert m == pytest.approx(ref.mD, rel=1e-12)
 
 
-@pytest.mark.parametrize("N,steps", [(256, 100), (128, 200), (1024, 50)])
+@pytest.mark.parametrize("N,steps", [(256, 100), (128, 200), (1024, 50), (4096, 12)])
 def test_mixed_vs_fp64_after_steps(N, steps):
     """Mixed-path fields after the given steps (dt from the oracle's CFL, checked against the
     device's) against the FP64 oracle stepped in lockstep; 1024^2 runs the fused transforms
-    and the packed hydro."""
-    ref = O.Disk(Nu=N, Nphi=N, eps=0.005, amp=1e-3, nthreads=8)
+    and the packed hydro, 4096^2 the four-pass u convolution and the four-step phi
+    transforms."""
+    ref = O.Disk(Nu=N, Nphi=N, eps=0.005, amp=1e-3, nthreads=os.cpu_count() or 8)
     S0 = ref.hyd.get("Sig").mean(axis=1, keepdims=True)
     with D.Disk(N, N, eps=0.005, amp=1e-3, precision="mixed") as d:
         d.init_standard()
