@@ -82,6 +82,8 @@ def parse():
     ap.add_argument("--batch-disks", type=int, default=256,
                     help="disks of the batched sweep measurement (0: skip it)")
     ap.add_argument("--batch-tlim", type=float, default=0.1, help="time the batched sweep advances")
+    ap.add_argument("--batch-grids", default="128,256,384,512", help="grid sizes the batch draws from")
+    ap.add_argument("--batch-seed", type=int, default=12345, help="seed of the batch's sweep-law draw")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -418,7 +420,8 @@ def batched_sweep(a, device, grouped=True):
     import diskgpu as D
     from diskgpu import sweep as S
     os.environ["DISKGPU_BATCH_GROUPS"] = "1" if grouped else "0"
-    pts = S.draw(a.batch_disks, seed=12345, grids=(128, 256, 384, 512))
+    grid_list = tuple(int(g) for g in a.batch_grids.split(","))
+    pts = S.draw(a.batch_disks, seed=a.batch_seed, grids=grid_list)
     params = [S.point_params(pt, "mixed", device) for pt in pts]
     with D.Batch(params) as b:
         b.init_standard()
