@@ -618,6 +618,26 @@ def main():
             dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
             e2e["value"] = world * zones * a.e2e_steps / float(t_e.item())
 
+    # ---- end to end through the device-resident loop: host state in, dg_advance over the
+    # same K steps' worth of simulated time with its mode records, final state out ----
+    e2e_loop = None
+    if a.e2e_steps > 0 and world == 1:
+        S, vR, vp = disk.get_state()
+        t_now, n_now = disk.time()
+        dt_est = t_now / max(n_now, 1)
+        span = dt_est * a.steps
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        disk.set_state(S, vR, vp)
+        recs, t1, n1 = disk.advance(span, dtout=span / 8)
+        S2, _, _ = disk.get_state()
+        el = time.perf_counter() - t0
+        e2e_loop = {"value": zones * n1 / el, "unit": UNIT, "steps": int(n1), "records": int(len(recs)),
+                    "h2d_bytes": 3 * 8 * zones, "d2h_bytes": 3 * 8 * zones + int(recs.nbytes),
+                    "how": "dg_set_state (FP64 host state) -> dg_advance over the simulated time of about K steps "
+                           "with mode records every eighth of it -> dg_get_state; wall clock; the state crosses PCIe "
+                           "once each way, not every step"}
+
     # ---- the plain FP64 path on the same disk, and a batched sweep (one rank) ----
     fp64 = batch = cufft = None
     if world == 1 and a.precision == "mixed":
@@ -664,7 +684,7 @@ def main():
             "data": "synthetic (standard heavy disk, seeded m=2 phase)", "config": cfg,
             "roofline": roof, "roofline_all": roof_all, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": kps * a.steps, "clocks": clk.summary(),
-            "repeats": spread(reps, a.steps) if reps else None,
+            "repeats": spread(reps, a.steps) if reps else None, "e2e_device_loop": e2e_loop,
             "fp64_same_disk": fp64, "cufft_gravity": cufft, "batched_sweep": batch, "conservation": drift,
         }
         print(json.dumps(line))
