@@ -279,9 +279,17 @@ __global__ void k_tab_kw(float *KW, const double2 *khat, int Nu, int Nphi) {
 // Tables of the four-step phi transforms at Nphi = 4096 (m = m1 + 64 m2, j = 64 j1 + j2):
 // PhA1[(m1, ri)][j1] = cos / -sin (2 pi m1 j1 / 64), the real-input 64-point DFT over j1;
 // PhB2i[j1][(m1, ri)] = cos / -sin (2 pi j1 m1 / 64) / N, the real part of the inverse
-// 64-point DFT over m1 with the inverse transform's 1 / N.
-__global__ void k_tab_ph4096(SplitBuf A1, SplitBuf B2i, int N) {
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 128 * 64; q += gridDim.x * blockDim.x) {
+// 64-point DFT over m1 with the inverse transform's 1 / N;
+// PhB2f[(m2, ro)][(ri, j2)]: the complex 64-point DFT W_64^{m2 j2} in real block form with
+// its K index planar (the real parts of the 64 inputs, then the imaginary parts).
+__global__ void k_tab_ph4096(SplitBuf A1, SplitBuf B2i, SplitBuf B2f, int N) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 128 * 128; q += gridDim.x * blockDim.x) {
+    const int row = q / 128, col = q % 128, m2 = row >> 1, ro = row & 1, ri = col >> 6, j2 = col & 63;
+    double sn, cs;
+    sincospi(2.0 * (double)((m2 * j2) % 64) / 64.0, &sn, &cs);
+    const double Fr = cs, Fi = -sn;  // W_64^{m2 j2} = exp(-2 pi i m2 j2 / 64)
+    put_split(B2f, q, ro == 0 ? (ri == 0 ? Fr : -Fi) : (ri == 0 ? Fi : Fr));
+    if (q >= 128 * 64) continue;
     {
       const int row = q / 64, j1 = q % 64, m1 = row >> 1, ri = row & 1;
       double sn, cs;
@@ -744,8 +752,7 @@ int dg_handle::mixed_init() {
       XK(alloc_split(X.PhB2f, (size_t)128 * 128)); XK(alloc_split(X.PhB1i, (size_t)128 * 128));
       XK(alloc_split(X.PhT, big)); XK(alloc_split(X.PhX, big)); XK(alloc_split(X.PhV, big));
       XK(dalloc(&X.twph, (size_t)64 * 64));
-      k_tab_ph4096<<<32, 256, 0, st>>>(X.PhA1, X.PhB2i, Nphi);
-      k_tab_cblock<<<64, 256, 0, st>>>(X.PhB2f, 64, 64, 64, -1);  // W_64^{m2 j2}
+      k_tab_ph4096<<<64, 256, 0, st>>>(X.PhA1, X.PhB2i, X.PhB2f, Nphi);
       k_tab_cblock<<<64, 256, 0, st>>>(X.PhB1i, 64, 64, 64, +1);  // W_64^{-j2 m2}
       k_tab_tw<<<64, 256, 0, st>>>(X.twph, 64, 64);                // W_4096^{m1 j2}
       XK(cudaGetLastError());
@@ -759,16 +766,17 @@ int dg_handle::mixed_init() {
                  make_map(&X.mPhB2i[0], X.PhB2i.hi, 64, 128, tc::BN) && make_map(&X.mPhB2i[1], X.PhB2i.lo, 64, 128, tc::BN) &&
                  make_map(&X.mPhT[0], X.PhT.hi, (uint64_t)64 * Nu, 128, tc::BM) &&
                  make_map(&X.mPhT[1], X.PhT.lo, (uint64_t)64 * Nu, 128, tc::BM) &&
-                 make_map(&X.mPhX[0], X.PhX.hi, (uint64_t)64 * Nu, 128, tc::BM) &&
-                 make_map(&X.mPhX[1], X.PhX.lo, (uint64_t)64 * Nu, 128, tc::BM) &&
-                 make_map(&X.mPhV[0], X.PhV.hi, (uint64_t)64 * Nu, 128, tc::BM) &&
-                 make_map(&X.mPhV[1], X.PhV.lo, (uint64_t)64 * Nu, 128, tc::BM);
+                 // X MN-major [(m2, ri)][(m1, i)]; V as [(i, m1, ri)][j2] (blocked MN-major A of Q2)
+                 make_map(&X.mPhX[0], X.PhX.hi, 128, (uint64_t)64 * Nu, 64) &&
+                 make_map(&X.mPhX[1], X.PhX.lo, 128, (uint64_t)64 * Nu, 64) &&
+                 make_map(&X.mPhV[0], X.PhV.hi, (uint64_t)128 * Nu, 64, 64) &&
+                 make_map(&X.mPhV[1], X.PhV.lo, (uint64_t)128 * Nu, 64, 64);
       if (!ok4) return fail(DG_ERR_CUDA, "mixed precision", "tensor map encoding failed (phi transforms at 4096)");
       XK((prepare_gemm<tc::kEpiPhiS1, false, true>()));
       XK((prepare_gemm<tc::kEpiPhiS2, false, false>()));
       XK((prepare_gemm<tc::kEpiI2ToX, false, false>()));
-      XK((prepare_gemm<tc::kEpiPhiQ1, false, false>()));
-      XK((prepare_gemm<tc::kEpiPhiQ2, false, false>()));
+      XK((prepare_gemm<tc::kEpiPhiQ1, true, false>()));
+      XK((prepare_gemm<tc::kEpiPhiQ2, true, false>()));
     }
     XK((prepare_gemm<tc::kEpiPhiToXin, false, false>()));
     XK((prepare_gemm<tc::kEpiTwiddleF1, false, true>()));
@@ -1278,7 +1286,7 @@ int dg_handle::mixed_gravity() {
       XK(launch_pdl(tc::k_phifwd, dim3(Nu / tc::kPfRows), dim3(tc::kPfThreads), tc::kPfSmem, st, X.mPA[0], X.mPA[1],
                     X.mPB[0], X.mPB[1], f));
     } else if (X.phi4096) {
-      // S1: real 64-point DFT over j1 (s read as [(i, j1)][j2]), x W_N^{j2 m1} -> T[(m1, i)][(j2, ri)]
+      // S1: real 64-point DFT over j1 (s read as [(i, j1)][j2]), x W_N^{j2 m1} -> T[(m1, i)][(ri, j2)]
       a.out_hi = X.PhT.hi; a.out_lo = X.PhT.lo; a.twiddle = X.twph;
       XK((gemm<tc::kEpiPhiS1, false, true>(X.mPhA1[0], X.mPhA1[1], X.mSxBlk[0], X.mSxBlk[1], 128, Nu * 64, 64, a,
                                              st, 0)));
@@ -1310,7 +1318,7 @@ int dg_handle::mixed_gravity() {
       a.out_hi = X.Ub.hi; a.out_lo = X.Ub.lo; a.table = nullptr;
       XK(gemm<tc::kEpiTwiddleI1>(X.mYk[0], X.mYk[1], X.mRGA[0], X.mRGA[1], nm * 64, 2 * A, 2 * A, a, st, X.ns[3]));
       // I2: inverse 64-point DFT over p2 (the 32 physical i2) -> Z[c][i], or at Nphi = 4096
-      // the full Hermitian spectrum X[(m % 64, i)][(m / 64, ri)] of the four-step inverse
+      // the full Hermitian spectrum X[(m / 64, ri)][(m % 64, i)] of the four-step inverse
       if (X.phi4096) {
         a.out_hi = X.PhX.hi; a.out_lo = X.PhX.lo;
         XK(gemm<tc::kEpiI2ToX>(X.mUb[0], X.mUb[1], X.mRGB[0], X.mRGB[1], nm * A, 64, 128, a, st, X.ns[4]));
@@ -1329,12 +1337,14 @@ int dg_handle::mixed_gravity() {
         X.hydro_kind == MixedState::kHydroPacked ? (Nphi + kTileJp - 1) / kTileJp : (Nphi + kTileJ - 1) / kTileJ;
     XK(prof_begin(DG_PROF_GRAV_PHI_INV));
     if (X.phi4096) {
-      // Q1: inverse 64-point DFT over m2, x W_N^{-j2 m1} -> V[(i, j2)][(m1, ri)]
+      // Q1: inverse 64-point DFT over m2 (X read MN-major), x W_N^{-j2 m1} -> V[(i, m1)][(ri, j2)]
       a.out_hi = X.PhV.hi; a.out_lo = X.PhV.lo; a.twiddle = X.twph;
-      XK(gemm<tc::kEpiPhiQ1>(X.mPhX[0], X.mPhX[1], X.mPhB1i[0], X.mPhB1i[1], 64 * Nu, 128, 128, a, st, 0));
+      XK((gemm<tc::kEpiPhiQ1, true, false>(X.mPhX[0], X.mPhX[1], X.mPhB1i[0], X.mPhB1i[1], 64 * Nu, 128, 128, a,
+                                            st, 0)));
       // Q2: real part of the inverse 64-point DFT over m1, / N, x (-G du dphi / sqrt(R))
       a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.row_scale = X.phiscale;
-      XK(gemm<tc::kEpiPhiQ2>(X.mPhV[0], X.mPhV[1], X.mPhB2i[0], X.mPhB2i[1], 64 * Nu, 64, 128, a, st, 0));
+      XK((gemm<tc::kEpiPhiQ2, true, false>(X.mPhV[0], X.mPhV[1], X.mPhB2i[0], X.mPhB2i[1], 64 * Nu, 64, 128, a,
+                                            st, 0)));
     } else if (X.fused_phi) {
       tc::PhiInvArgs f{X.Zt.hi, X.Zt.lo, X.twphi, X.phiscale, X.dPhi, Nphi, &ctl->status, rp, rp_n, rp_val};
       XK(launch_pdl(tc::k_phiinv, dim3(Nu / tc::kPiRows), dim3(tc::kPiThreads), tc::kPiSmem, st, X.mIA[0], X.mIA[1],

@@ -50,11 +50,15 @@ enum EpiMode : int {
   kEpiStoreBounded = 10,  // D -> out_f32[row][col] for row < lim_m, col < lim_n (weight gradients)
   // factored phi transforms at Nphi = 4096 = 64 x 64 (j = 64 j1 + j2, m = m1 + 64 m2;
   // mixed.cu documents the passes).  The S1 product reads its B operand (the gravity
-  // operand s[i][64 j1 + j2] as the [(i, j1)][j2] matrix) in 64 x 64 blocks per row i.
-  kEpiPhiS1 = 11,       // rows (m1, ri), cols (i, j2): x W_N^{j2 m1} -> T[(m1, i)][(j2, ri)]
+  // operand s[i][64 j1 + j2] as the [(i, j1)][j2] matrix) in 64 x 64 blocks per row i, the
+  // Q2 product its A operand (V[(i, m1)][(ri, j2)] as [(i, m1, ri)][j2]) in 128 x 64
+  // blocks per row i: both MN-major with the block's rows as K.
+  // Layouts chosen so that every epilogue stores contiguous runs: T and V hold the real
+  // and imaginary parts as two 64-column planes of each row, X is stored MN-major.
+  kEpiPhiS1 = 11,       // rows (m1, ri), cols (i, j2): x W_N^{j2 m1} -> T[(m1, i)][(ri, j2)]
   kEpiPhiS2 = 12,       // rows (m1, i), cols (m2, ri): modes m <= N/2 -> Xin[(i2, ri)][(m, i1)]
-  kEpiI2ToX = 13,       // rows (m, i1), cols (i2, ri): X and its conjugate -> X[(m % 64, i)][(m / 64, ri)]
-  kEpiPhiQ1 = 14,       // rows (m1, i), cols (j2, ri): x W_N^{-j2 m1} -> V[(i, j2)][(m1, ri)]
+  kEpiI2ToX = 13,       // rows (m, i1), cols (i2, ri): X and its conjugate -> X[(m / 64, ri)][(m % 64, i)]
+  kEpiPhiQ1 = 14,       // rows (m1, i), cols (j2, ri): x W_N^{-j2 m1} -> V[(i, m1)][(ri, j2)]
   kEpiPhiQ2 = 15,       // rows (i, j2), cols j1: x row_scale[i] -> out_f32[i][64 j1 + j2]
 };
 
@@ -376,28 +380,37 @@ __device__ __forceinline__ void epi_phi4096(const GemmArgs &a, int row, int col,
     a.out_hi[k] = h;
     a.out_lo[k] = l;
   };
-  auto put2 = [&](size_t k, float x, float y) {  // (x, y) at k, k + 1 (k even): one word per plane
-    __nv_bfloat16 h0, l0, h1, l1;
-    split_bf16(x, h0, l0);
-    split_bf16(y, h1, l1);
-    *reinterpret_cast<uint32_t *>(a.out_hi + k) =
-        (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-    *reinterpret_cast<uint32_t *>(a.out_lo + k) =
-        (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
-  };
   if (MODE == kEpiPhiS1) {
-    // rows (m1, ri): re / im of one m1 in lanes l, l^1; cols (i, j2), the chunk inside one i
+    // rows (m1, ri): re / im of one m1 in lanes l, l^1; cols (i, j2), the chunk inside one i;
+    // each lane stores its 32 values of one plane contiguously
     const int m1 = row >> 1, ri = row & 1;
     const int i = col >> 6, j2b = col & 63;
-    const size_t base = ((size_t)m1 * Nu + i) * 128 + ri;
     const float2 *tw = a.twiddle + m1 * 64 + j2b;
+    uint32_t ph[16], pl[16];
 #pragma unroll
-    for (int q = 0; q < 32; ++q) {
-      const float v = __uint_as_float(r[q]);
-      const float o = __shfl_xor_sync(0xffffffffu, v, 1);
-      const float re = ri ? o : v, im = ri ? v : o;
-      const float2 w = __ldg(tw + q);
-      put(base + 2 * (j2b + q), ri ? (re * w.y + im * w.x) : (re * w.x - im * w.y));
+    for (int q = 0; q < 32; q += 2) {
+      float out[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const float v = __uint_as_float(r[q + e]);
+        const float o = __shfl_xor_sync(0xffffffffu, v, 1);
+        const float re = ri ? o : v, im = ri ? v : o;
+        const float2 w = __ldg(tw + q + e);
+        out[e] = ri ? (re * w.y + im * w.x) : (re * w.x - im * w.y);
+      }
+      __nv_bfloat16 h0, l0, h1, l1;
+      split_bf16(out[0], h0, l0);
+      split_bf16(out[1], h1, l1);
+      ph[q >> 1] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+      pl[q >> 1] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+    }
+    const size_t base = ((size_t)m1 * Nu + i) * 128 + ri * 64 + j2b;
+    uint4 *oh = reinterpret_cast<uint4 *>(a.out_hi + base);
+    uint4 *ol = reinterpret_cast<uint4 *>(a.out_lo + base);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      oh[q] = make_uint4(ph[4 * q], ph[4 * q + 1], ph[4 * q + 2], ph[4 * q + 3]);
+      ol[q] = make_uint4(pl[4 * q], pl[4 * q + 1], pl[4 * q + 2], pl[4 * q + 3]);
     }
   } else if (MODE == kEpiPhiS2) {
     // rows (m1, i), cols (m2, ri) pairs in-thread -> the u stage's operand Xin
@@ -421,22 +434,51 @@ __device__ __forceinline__ void epi_phi4096(const GemmArgs &a, int row, int col,
       const size_t i = (size_t)i1 + (size_t)A * (i2b + (q >> 1));
       const float re = __uint_as_float(r[q]);
       const float im = (m == 0 || m == half) ? 0.f : __uint_as_float(r[q + 1]);
-      put2(((size_t)(m & 63) * Nu + i) * 128 + 2 * (m >> 6), re, im);
+      // MN-major: row (m2, ri), column (m1, i): consecutive lanes (i1) store consecutive words
+      const size_t ldx = (size_t)64 * Nu;
+      const size_t c0 = (size_t)(m & 63) * Nu + i;
+      put((size_t)(2 * (m >> 6)) * ldx + c0, re);
+      put((size_t)(2 * (m >> 6) + 1) * ldx + c0, im);
       if (m != 0 && m != half) {
         const int mc = N - m;
-        put2(((size_t)(mc & 63) * Nu + i) * 128 + 2 * (mc >> 6), re, -im);
+        const size_t c1 = (size_t)(mc & 63) * Nu + i;
+        put((size_t)(2 * (mc >> 6)) * ldx + c1, re);
+        put((size_t)(2 * (mc >> 6) + 1) * ldx + c1, -im);
       }
     }
   } else if (MODE == kEpiPhiQ1) {
-    // rows (m1, i), cols (j2, ri) pairs in-thread: x conj(W_N^{m1 j2}) -> V[(i, j2)][(m1, ri)]
+    // rows (m1, i), cols (j2, ri) pairs in-thread: x conj(W_N^{m1 j2}) -> V[(i, m1)][(ri, j2)],
+    // 16 contiguous j2 per plane
     const int m1 = row / Nu, i = row - m1 * Nu;
     const int j2b = col >> 1;
     const float2 *tw = a.twiddle + m1 * 64 + j2b;
+    float ore[16], oim[16];
 #pragma unroll
     for (int q = 0; q < 32; q += 2) {
       const float re = __uint_as_float(r[q]), im = __uint_as_float(r[q + 1]);
       const float2 w = __ldg(tw + (q >> 1));
-      put2(((size_t)i * 64 + j2b + (q >> 1)) * 128 + 2 * m1, re * w.x + im * w.y, im * w.x - re * w.y);
+      ore[q >> 1] = re * w.x + im * w.y;
+      oim[q >> 1] = im * w.x - re * w.y;
+    }
+    const size_t base = ((size_t)i * 64 + m1) * 128 + j2b;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const float *src = e ? oim : ore;
+      uint32_t ph[8], pl[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        __nv_bfloat16 h0, l0, h1, l1;
+        split_bf16(src[2 * q], h0, l0);
+        split_bf16(src[2 * q + 1], h1, l1);
+        ph[q] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+        pl[q] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+      }
+      uint4 *oh = reinterpret_cast<uint4 *>(a.out_hi + base + 64 * e);
+      uint4 *ol = reinterpret_cast<uint4 *>(a.out_lo + base + 64 * e);
+      oh[0] = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+      oh[1] = make_uint4(ph[4], ph[5], ph[6], ph[7]);
+      ol[0] = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+      ol[1] = make_uint4(pl[4], pl[5], pl[6], pl[7]);
     }
   } else if (MODE == kEpiPhiQ2) {
     // rows (i, j2), cols j1: dPhi[i][64 j1 + j2] (lanes: consecutive j2, so coalesced)
@@ -551,7 +593,12 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap *pAh, const CUtensor
       if (abort_flag) break;
       uint8_t *st = smem + s * kStageBytes;
       mbar_arrive_expect_tx(&full_bar[s], kStageBytes);
-      if (A_MN) {  // [K][M] in global: two 64-wide M chunks of 64 K rows
+      if (A_MN && MODE == kEpiPhiQ2) {  // V as [(i, m1, ri)][j2]: M chunk c = row i = m0 / 64 + c
+        tma_load_2d(st, pAh, &full_bar[s], 0, (m0 / 64) * 128 + kc * BK);
+        tma_load_2d(st + kTileA / 2, pAh, &full_bar[s], 0, (m0 / 64 + 1) * 128 + kc * BK);
+        tma_load_2d(st + kTileA, pAl, &full_bar[s], 0, (m0 / 64) * 128 + kc * BK);
+        tma_load_2d(st + kTileA + kTileA / 2, pAl, &full_bar[s], 0, (m0 / 64 + 1) * 128 + kc * BK);
+      } else if (A_MN) {  // [K][M] in global: two 64-wide M chunks of 64 K rows
         tma_load_2d(st, pAh, &full_bar[s], m0, kc * BK);
         tma_load_2d(st + kTileA / 2, pAh, &full_bar[s], m0 + 64, kc * BK);
         tma_load_2d(st + kTileA, pAl, &full_bar[s], m0, kc * BK);
