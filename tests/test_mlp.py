@@ -75,7 +75,8 @@ def test_shipped_surrogate_on_gpu_matches_oracle():
 
     from diskgpu.surrogate import TRAINED, lka98_features, read_surrogate
     d = read_surrogate(TRAINED)
-    with np.load(os.path.join(os.path.dirname(TRAINED), "sweep_128_dataset.npz")) as z:
+    grid = int(d["report"].get("grid", 128))
+    with np.load(os.path.join(os.path.dirname(TRAINED), f"sweep_{grid}_dataset.npz")) as z:
         X = np.concatenate([z["data"][-51:, :4], lka98_features()])
     sur = Surrogate.load(TRAINED)
     got = sur.predict(X)

@@ -21,7 +21,12 @@ import mlp_ref as R
 from diskgpu.surrogate import TRAINED, lka98_features, lka98_omega_guess, read_surrogate
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DATASET = os.path.join(os.path.dirname(TRAINED), "sweep_128_dataset.npz")
+
+
+def _dataset():
+    """The training sweep the shipped network was trained on (its grid is in the report)."""
+    grid = int(read_surrogate(TRAINED)["report"].get("grid", 128))
+    return os.path.join(os.path.dirname(TRAINED), f"sweep_{grid}_dataset.npz")
 
 
 def _predict(d, X):
@@ -32,7 +37,7 @@ def _predict(d, X):
 
 def test_shipped_surrogate_beats_constant_guess_on_held_out_runs():
     d = read_surrogate(TRAINED)
-    with np.load(DATASET) as z:
+    with np.load(_dataset()) as z:
         data = z["data"]
     X, Y = data[:, :4], data[:, 5:8]
     ok = np.all(np.isfinite(Y), axis=1)
