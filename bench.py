@@ -17,7 +17,8 @@ time and, with per-kernel events, the roofline of every kernel of the step.  On 
 line also carries `fp64_same_disk` (the plain FP64 path on the same disk, timed over the
 same K steps, and the mixed/FP64 ratio the metric names), `cufft_gravity` (the same padded
 convolution through cuFFT, as a timing comparison only) and `batched_sweep` (256 disks of
-the sweep law, grids 128^2..512^2, advanced together by dg_batch).
+the sweep law, grids 128^2..512^2, advanced together by dg_batch; inside it `batched_1024`,
+16 sweep-law disks all at 1024^2, and their ratio to the plain FP64 path at 1024^2).
 
 --impl reference times the reference's own CPU implementation (diskfft/src hydro.hpp +
 kalnajs.hpp compiled unmodified against the FFTW-API shim, with the reference Makefile's
@@ -84,6 +85,9 @@ def parse():
     ap.add_argument("--batch-tlim", type=float, default=0.1, help="time the batched sweep advances")
     ap.add_argument("--batch-grids", default="128,256,384,512", help="grid sizes the batch draws from")
     ap.add_argument("--batch-seed", type=int, default=12345, help="seed of the batch's sweep-law draw")
+    ap.add_argument("--batch1024-disks", type=int, default=16,
+                    help="disks of the batched 1024^2 measurement (sweep-law physics, every grid 1024^2; 0: skip)")
+    ap.add_argument("--batch1024-tlim", type=float, default=0.05, help="time the batched 1024^2 disks advance")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -411,42 +415,47 @@ def cufft_gravity(a, device, flush, disk64_potential):
     return out
 
 
-def batched_sweep(a, device, grouped=True):
+def batched_sweep(a, device, grouped=True, ndisks=None, grids=None, tlim=None):
     """Throughput of a batched sweep: `--batch-disks` disks drawn by the sweep law (grids
     128^2..512^2, Q_min, M_d/M_*, softening/r, Gamma; seed 12345), mixed precision, advanced
     together by dg_batch (one graph launch advances every disk 64 steps; same-grid disks
-    as groups, one launch per kernel, unless grouped is False)."""
+    as groups, one launch per kernel, unless grouped is False).  ndisks / grids / tlim
+    override the batch options (the batched 1024^2 measurement)."""
     import torch
     import diskgpu as D
     from diskgpu import sweep as S
     os.environ["DISKGPU_BATCH_GROUPS"] = "1" if grouped else "0"
-    grid_list = tuple(int(g) for g in a.batch_grids.split(","))
-    pts = S.draw(a.batch_disks, seed=a.batch_seed, grids=grid_list)
+    grid_list = grids or tuple(int(g) for g in a.batch_grids.split(","))
+    tlim = a.batch_tlim if tlim is None else tlim
+    pts = S.draw(ndisks or a.batch_disks, seed=a.batch_seed, grids=grid_list)
     params = [S.point_params(pt, "mixed", device) for pt in pts]
     with D.Batch(params) as b:
         b.init_standard()
         _, _, s0 = b.advance(0.01, steps_per_launch=64)  # captures the graph
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        _, _, s1 = b.advance(0.01 + a.batch_tlim, steps_per_launch=64)
+        _, _, s1 = b.advance(0.01 + tlim, steps_per_launch=64)
         el = time.perf_counter() - t0
     os.environ.pop("DISKGPU_BATCH_GROUPS", None)
     zu = float(sum(pt.N * pt.N * (int(x1) - int(x0)) for pt, x0, x1 in zip(pts, s0, s1)))
-    # split-BF16 dense DFT products of a disk step: 6 N^3 (phi) + 12 N^3 + 12 N^3 (u) + 6 N^3 (inverse phi)
-    flops = float(sum(36.0 * pt.N ** 3 * (int(x1) - int(x0)) for pt, x0, x1 in zip(pts, s0, s1)))
+    # executed split-BF16 gravity flops of a disk step (dense products up to 512^2: 36 N^3;
+    # the fused factored transforms at 1024^2)
+    step_flops = {N: float(sum(p[3] for p in gravity_parts("mixed", N, N))) for N in set(pt.N for pt in pts)}
+    flops = float(sum(step_flops[pt.N] * (int(x1) - int(x0)) for pt, x0, x1 in zip(pts, s0, s1)))
     grids = {}
     for pt in pts:
         grids[pt.N] = grids.get(pt.N, 0) + 1
     hbm_peak, tc_peak, kind = measured_peaks()
     hyd = 32.0 * zu / el / 1e9
     return {"value": zu / el, "unit": UNIT, "disks": len(pts), "grids": {f"{k}^2": v for k, v in sorted(grids.items())},
-            "zone_updates": zu, "seconds": el, "sim_time": a.batch_tlim, "grouped": grouped,
+            "zone_updates": zu, "seconds": el, "sim_time": tlim, "grouped": grouped,
             "hydro_algorithmic_GBps": hyd, "hydro_frac_of_hbm": hyd / hbm_peak,
             "gravity_executed_TFLOPs": flops / el / 1e12, "gravity_frac_of_tensor": flops / el / 1e12 / tc_peak,
             "peak_kind": kind,
             "how": "wall clock around dg_batch_advance (graph launches of 64 steps per disk, the host reads "
                    "every disk's control block between launches); algorithmic rates over the whole job: 32 B per "
-                   "zone-update for the hydro, 36 N^3 executed flops per disk-step for the dense gravity products"}
+                   "zone-update for the hydro, the executed split-BF16 flops of each disk-step's gravity products "
+                   "(36 N^3 for the dense products)"}
 
 
 TRAFFIC_KEYS = {"hydro": "hydro", "grav_phi_fwd": "grav_phi_fwd", "grav_u": "grav_u", "grav_phi_inv": "grav_phi_inv"}
@@ -659,6 +668,14 @@ def main():
         if a.batch_disks > 0:
             batch = batched_sweep(a, local, grouped=True)
             batch["ungrouped"] = batched_sweep(a, local, grouped=False)["value"]
+        if a.batch1024_disks > 0:
+            b1k = batched_sweep(a, local, grouped=True, ndisks=a.batch1024_disks, grids=(1024,),
+                                tlim=a.batch1024_tlim)
+            b1k["ungrouped"] = batched_sweep(a, local, grouped=False, ndisks=a.batch1024_disks, grids=(1024,),
+                                             tlim=a.batch1024_tlim)["value"]
+            if fp64 is not None and N == 1024:
+                b1k["over_fp64_plain_1024"] = b1k["value"] / fp64["value"]
+            batch = dict(batch or {}, batched_1024=b1k)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

@@ -1515,10 +1515,11 @@ int dg_handle::mixed_potential(const double *dSig, double *dOut) {
 // ---------------------------------------------------------------------------------
 // Disk groups of a batched sweep (batch.cu): disks of one grid, Gamma class, hydro form and
 // product pipeline depths advance with one launch per kernel for the whole group (the
-// disk in blockIdx.z).  Each disk keeps its own state, khat table, row tables, control
-// block and dt; the DFT tables, identical for one grid, are the lead disk's.  A disk's
-// tiles run exactly the code of its lone step, so a grouped step equals the lone one bit
-// for bit.
+// disk in blockIdx.z, or blockIdx.y for the fused 1024^2 transforms).  Each disk keeps its
+// own state, khat table, row tables, control block and dt; the DFT tables, identical for
+// one grid, are the lead disk's.  A disk's tiles run exactly the code of its lone step, so
+// a grouped step equals the lone one bit for bit (the lone step's row-tile hand-over
+// between the hydro sweep and the phi transforms only orders the same work differently).
 
 struct MixedGroup {
   std::vector<dg_handle *> disks;
@@ -1530,17 +1531,24 @@ struct MixedGroup {
   int nsm = 148;
   tc::GemmDisk *gd[4] = {nullptr, nullptr, nullptr, nullptr};  // per product: one entry per disk
   HydroDisk *hd = nullptr;
+  // 1024^2 disks: the fused phi transform, u convolution and inverse phi transform
+  bool fused = false;
+  tc::PhiFwdArgs *pf = nullptr;
+  tc::UconvDisk *uc = nullptr;
+  tc::PhiInvArgs *pi = nullptr;
 };
 
 std::string mixed_group_key(const dg_handle *h) {
   if (!h || h->p.precision != DG_PREC_MIXED || !h->p.selfgrav || !h->mx || !h->mx->tables_ready ||
-      h->mx->factored || !h->have_state)
+      !h->have_state)
     return std::string();
   const MixedState &X = *h->mx;
+  // dense products, or the fused 1024^2 transforms (the other factored forms step alone)
+  if (X.factored && !X.fused_phi) return std::string();
   if (X.hydro_kind != MixedState::kHydroPacked && X.hydro_kind != MixedState::kHydroTile) return std::string();
   char b[160];
-  snprintf(b, sizeof b, "%d:%d:%d:%d:%d:%d,%d,%d,%d", h->dev, X.Nu, X.Nphi, X.rows.gamma2, X.hydro_kind, X.ns[0],
-           X.ns[1], X.ns[2], X.ns[5]);
+  snprintf(b, sizeof b, "%d:%d:%d:%d:%d:%d:%d,%d,%d,%d", h->dev, X.Nu, X.Nphi, X.fused_phi ? 1 : 0, X.rows.gamma2,
+           X.hydro_kind, X.ns[0], X.ns[1], X.ns[2], X.ns[5]);
   return std::string(b);
 }
 
@@ -1577,10 +1585,31 @@ static int group_launch(MixedGroup *g, cudaStream_t st, bool prepare) {
   MixedState &X = *L->mx;
   const int Nu = X.Nu, Nphi = X.Nphi, G = (int)g->disks.size();
   cudaError_t e;
+  if (g->fused) {
+    // phi transform -> Xin, u convolution (F1 F2 I1 I2) -> Zt, inverse phi transform -> dPhi
+    if (prepare) {
+      e = smem_attrs((const void *)tc::k_phifwd_group, tc::kPfSmem);
+      if (e == cudaSuccess) e = smem_attrs((const void *)tc::k_uconv_group, tc::kUcSmem);
+      if (e == cudaSuccess) e = smem_attrs((const void *)tc::k_phiinv_group, tc::kPiSmem);
+      if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: fused transforms", cudaGetErrorString(e));
+    } else {
+      e = launch_pdl(tc::k_phifwd_group, dim3(Nu / tc::kPfRows, G), dim3(tc::kPfThreads), tc::kPfSmem, st,
+                     X.mPA[0], X.mPA[1], X.mPB[0], X.mPB[1], (const tc::PhiFwdArgs *)g->pf);
+      if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: phi transform", cudaGetErrorString(e));
+      e = launch_pdl(tc::k_uconv_group, dim3(X.nm / tc::kUcModes, G), dim3(tc::kUcThreads), tc::kUcSmem, st,
+                     X.mRB[0], X.mRB[1], X.mRA[0], X.mRA[1], X.mRGA[0], X.mRGA[1], X.mRGB[0], X.mRGB[1],
+                     (const tc::UconvDisk *)g->uc);
+      if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: u convolution", cudaGetErrorString(e));
+      e = launch_pdl(tc::k_phiinv_group, dim3(Nu / tc::kPiRows, G), dim3(tc::kPiThreads), tc::kPiSmem, st,
+                     X.mIA[0], X.mIA[1], X.mIB[0], X.mIB[1], (const tc::PhiInvArgs *)g->pi);
+      if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: inverse phi transform", cudaGetErrorString(e));
+    }
+  }
   // G1: X1[c][i] = Fphi[c][:] . Sx[i][:];  G2: Wt[c][p] = KW[c][p] X1[c][:] . Cu[p][:];
   // G3: Z[i][c] = CuT[i][:] . Wt[c][:];    G4: dPhi[i][j] = phiscale[i] Z[i][:] . Gphi[j][:]
-  e = gemm_group<tc::kEpiSplit, false, false, false>(X.mFphi[0], X.mFphi[1], g->gd[0], G, Nphi, Nu, Nphi, st, g->ns[0],
+  if (!g->fused) e = gemm_group<tc::kEpiSplit, false, false, false>(X.mFphi[0], X.mFphi[1], g->gd[0], G, Nphi, Nu, Nphi, st, g->ns[0],
                                                        prepare, g->persist, g->nsm);
+  if (!g->fused) {
   if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: phi DFT", cudaGetErrorString(e));
   e = gemm_group<tc::kEpiSplitScaled, false, false, true>(X.mCu[0], X.mCu[1], g->gd[1], G, Nphi, 2 * Nu, Nu, st,
                                                           g->ns[1], prepare, g->persist, g->nsm);
@@ -1591,6 +1620,7 @@ static int group_launch(MixedGroup *g, cudaStream_t st, bool prepare) {
   e = gemm_group<tc::kEpiRowScaleF32, false, false, true>(X.mGphi[0], X.mGphi[1], g->gd[3], G, Nu, Nphi, Nphi, st,
                                                           g->ns[5], prepare, g->persist, g->nsm);
   if (e != cudaSuccess) return L->fail(DG_ERR_CUDA, "batch group: inverse phi DFT", cudaGetErrorString(e));
+  }
   const bool packed = g->kind == MixedState::kHydroPacked;
   auto hk = packed ? (g->g2 ? k_hydro32p_group<true> : k_hydro32p_group<false>)
                    : (g->g2 ? k_hydro32t_group<true> : k_hydro32t_group<false>);
@@ -1616,7 +1646,16 @@ void mixed_group_destroy(MixedGroup *g) {
   for (tc::GemmDisk *p : g->gd)
     if (p) cudaFree(p);
   if (g->hd) cudaFree(g->hd);
+  if (g->pf) cudaFree(g->pf);
+  if (g->uc) cudaFree(g->uc);
+  if (g->pi) cudaFree(g->pi);
   delete g;
+}
+
+template <class T>
+static cudaError_t upload(T **dst, const std::vector<T> &v) {
+  cudaError_t e = cudaMalloc(dst, sizeof(T) * v.size());
+  return e == cudaSuccess ? cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice) : e;
 }
 
 MixedGroup *mixed_group_create(const std::vector<dg_handle *> &disks, std::string *err) {
@@ -1641,13 +1680,40 @@ MixedGroup *mixed_group_create(const std::vector<dg_handle *> &disks, std::strin
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->lead->dev) == cudaSuccess && nsm > 0)
       g->nsm = nsm;
   }
+  g->fused = XL.fused_phi;
   const int G = (int)disks.size(), Nu = XL.Nu, Nphi = XL.Nphi;
   std::vector<tc::GemmDisk> gd[4];
   std::vector<HydroDisk> hd(G);
-  for (int q = 0; q < 4; ++q) gd[q].resize(G);
+  std::vector<tc::PhiFwdArgs> pf;
+  std::vector<tc::UconvDisk> uc;
+  std::vector<tc::PhiInvArgs> pi;
+  if (!g->fused)
+    for (int q = 0; q < 4; ++q) gd[q].resize(G);
   for (int k = 0; k < G; ++k) {
     dg_handle *h = disks[k];
     MixedState &X = *h->mx;
+    HydroDisk &d = hd[k];
+    for (int b = 0; b < 2; ++b) {
+      d.tmS[b] = X.mSig[b]; d.tmU[b] = X.mU[b]; d.tmW[b] = X.mW[b];
+      d.sig[b] = X.sig[b]; d.u[b] = X.u[b]; d.w[b] = X.w[b];
+    }
+    d.tmP = X.mPhi;
+    d.dPhi = X.dPhi;
+    d.Sx = SplitBf16{X.Sx.hi, X.Sx.lo};
+    d.ctl = h->ctl;
+    d.g = X.rows;
+    if (g->fused) {
+      // the lone step's arguments without the row-tile hand-over (tables: the lead's)
+      pf.push_back(tc::PhiFwdArgs{X.Sx.hi, X.Sx.lo, XL.twphi, X.Xin.hi, X.Xin.lo, X.nm * X.fa, Nphi,
+                                  &h->ctl->status, nullptr});
+      tc::UconvDisk u{};
+      u.xh = X.mXin[0]; u.xl = X.mXin[1];
+      u.a = tc::UconvArgs{XL.twp, X.khm, X.Z.hi, X.Z.lo, Nu, Nphi, &h->ctl->status, X.Zt.hi, X.Zt.lo};
+      uc.push_back(u);
+      pi.push_back(tc::PhiInvArgs{X.Zt.hi, X.Zt.lo, XL.twphi, X.phiscale, X.dPhi, Nphi, &h->ctl->status, nullptr,
+                                  0, 0});
+      continue;
+    }
     tc::GemmArgs a{};
     a.status = &h->ctl->status;
     // G1: per-disk B = Sx -> X1
@@ -1663,19 +1729,14 @@ MixedGroup *mixed_group_create(const std::vector<dg_handle *> &disks, std::strin
     a.M = Nu; a.N = Nphi; a.K = Nphi; a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.ldo = Nphi;
     a.row_scale = X.phiscale;
     gd[3][k].hi = X.mZ[0]; gd[3][k].lo = X.mZ[1]; gd[3][k].args = a;
-    HydroDisk &d = hd[k];
-    for (int b = 0; b < 2; ++b) {
-      d.tmS[b] = X.mSig[b]; d.tmU[b] = X.mU[b]; d.tmW[b] = X.mW[b];
-      d.sig[b] = X.sig[b]; d.u[b] = X.u[b]; d.w[b] = X.w[b];
-    }
-    d.tmP = X.mPhi;
-    d.dPhi = X.dPhi;
-    d.Sx = SplitBf16{X.Sx.hi, X.Sx.lo};
-    d.ctl = h->ctl;
-    d.g = X.rows;
   }
   cudaError_t e = cudaSetDevice(g->lead->dev);
-  for (int q = 0; q < 4 && e == cudaSuccess; ++q) {
+  if (g->fused) {
+    if (e == cudaSuccess) e = upload(&g->pf, pf);
+    if (e == cudaSuccess) e = upload(&g->uc, uc);
+    if (e == cudaSuccess) e = upload(&g->pi, pi);
+  }
+  for (int q = 0; q < 4 && e == cudaSuccess && !g->fused; ++q) {
     e = cudaMalloc(&g->gd[q], sizeof(tc::GemmDisk) * G);
     if (e == cudaSuccess)
       e = cudaMemcpy(g->gd[q], gd[q].data(), sizeof(tc::GemmDisk) * G, cudaMemcpyHostToDevice);

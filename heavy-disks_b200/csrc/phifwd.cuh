@@ -47,9 +47,7 @@ struct PhiFwdArgs {
   const int *rowpend;
 };
 
-__global__ void __launch_bounds__(kPfThreads, 2)
-    k_phifwd(const __grid_constant__ CUtensorMap tCh, const __grid_constant__ CUtensorMap tCl,
-             const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl, PhiFwdArgs a) {
+__device__ __forceinline__ void phifwd_cta(const CUtensorMap *pCh, const CUtensorMap *pCl, const CUtensorMap *pBh, const CUtensorMap *pBl, const PhiFwdArgs &a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *sm = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ __align__(8) uint64_t bar_in, bar_mma;
@@ -81,10 +79,10 @@ __global__ void __launch_bounds__(kPfThreads, 2)
 
   if (threadIdx.x == 0) {  // constant operands: they do not depend on the previous kernel
     mbar_arrive_expect_tx(&bar_in, 32768);
-    tma_load_2d(sm + kPfC, &tCh, &bar_in, 0, 0);
-    tma_load_2d(sm + kPfC + 8192, &tCl, &bar_in, 0, 0);
-    tma_load_2d(sm + kPfB, &tBh, &bar_in, 0, 0);
-    tma_load_2d(sm + kPfB + 8192, &tBl, &bar_in, 0, 0);
+    tma_load_2d(sm + kPfC, pCh, &bar_in, 0, 0);
+    tma_load_2d(sm + kPfC + 8192, pCl, &bar_in, 0, 0);
+    tma_load_2d(sm + kPfB, pBh, &bar_in, 0, 0);
+    tma_load_2d(sm + kPfB + 8192, pBl, &bar_in, 0, 0);
   }
   // the source comes from the hydro step before this kernel (Xin's last reader, the u
   // convolution of the previous step, completed before that hydro step started)
@@ -196,6 +194,24 @@ __global__ void __launch_bounds__(kPfThreads, 2)
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, kPfTmemCols);
+}
+
+__global__ void __launch_bounds__(kPfThreads, 2)
+    k_phifwd(const __grid_constant__ CUtensorMap tCh,
+    const __grid_constant__ CUtensorMap tCl,
+    const __grid_constant__ CUtensorMap tBh,
+    const __grid_constant__ CUtensorMap tBl, PhiFwdArgs a) {
+  phifwd_cta(&tCh, &tCl, &tBh, &tBl, a);
+}
+
+// The same for a group of disks of one grid (batched sweeps): blockIdx.y is the disk, whose
+// arguments come from a device array.
+__global__ void __launch_bounds__(kPfThreads, 2)
+    k_phifwd_group(const __grid_constant__ CUtensorMap tCh,
+    const __grid_constant__ CUtensorMap tCl,
+    const __grid_constant__ CUtensorMap tBh,
+    const __grid_constant__ CUtensorMap tBl, const PhiFwdArgs *__restrict__ disks) {
+  phifwd_cta(&tCh, &tCl, &tBh, &tBl, disks[blockIdx.y]);
 }
 
 }  // namespace tc

@@ -51,9 +51,7 @@ struct PhiInvArgs {
   int rp_n, rp_val;
 };
 
-__global__ void __launch_bounds__(kPiThreads, 2)
-    k_phiinv(const __grid_constant__ CUtensorMap tCh, const __grid_constant__ CUtensorMap tCl,
-             const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl, PhiInvArgs a) {
+__device__ __forceinline__ void phiinv_cta(const CUtensorMap *pCh, const CUtensorMap *pCl, const CUtensorMap *pBh, const CUtensorMap *pBl, const PhiInvArgs &a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *sm = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ __align__(8) uint64_t bar_in, bar_mma;
@@ -86,10 +84,10 @@ __global__ void __launch_bounds__(kPiThreads, 2)
 
   if (threadIdx.x == 0) {  // constant operands: they do not depend on the previous kernel
     mbar_arrive_expect_tx(&bar_in, 16384 + 8192);
-    tma_load_2d(sm + kPiC, &tCh, &bar_in, 0, 0);
-    tma_load_2d(sm + kPiC + 8192, &tCl, &bar_in, 0, 0);
-    tma_load_2d(sm + kPiB, &tBh, &bar_in, 0, 0);
-    tma_load_2d(sm + kPiB + 4096, &tBl, &bar_in, 0, 0);
+    tma_load_2d(sm + kPiC, pCh, &bar_in, 0, 0);
+    tma_load_2d(sm + kPiC + 8192, pCl, &bar_in, 0, 0);
+    tma_load_2d(sm + kPiB, pBh, &bar_in, 0, 0);
+    tma_load_2d(sm + kPiB + 4096, pBl, &bar_in, 0, 0);
   }
   pdl_wait();  // Zt comes from the previous kernel; the potential's last reader (the hydro
                // step of the previous time step) completed before that kernel started
@@ -194,6 +192,24 @@ __global__ void __launch_bounds__(kPiThreads, 2)
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, kPiTmemCols);
+}
+
+__global__ void __launch_bounds__(kPiThreads, 2)
+    k_phiinv(const __grid_constant__ CUtensorMap tCh,
+    const __grid_constant__ CUtensorMap tCl,
+    const __grid_constant__ CUtensorMap tBh,
+    const __grid_constant__ CUtensorMap tBl, PhiInvArgs a) {
+  phiinv_cta(&tCh, &tCl, &tBh, &tBl, a);
+}
+
+// The same for a group of disks of one grid (batched sweeps): blockIdx.y is the disk, whose
+// arguments come from a device array.
+__global__ void __launch_bounds__(kPiThreads, 2)
+    k_phiinv_group(const __grid_constant__ CUtensorMap tCh,
+    const __grid_constant__ CUtensorMap tCl,
+    const __grid_constant__ CUtensorMap tBh,
+    const __grid_constant__ CUtensorMap tBl, const PhiInvArgs *__restrict__ disks) {
+  phiinv_cta(&tCh, &tCl, &tBh, &tBl, disks[blockIdx.y]);
 }
 
 }  // namespace tc

@@ -90,12 +90,7 @@ __device__ __forceinline__ void uc_stage_sync() {
   tc_fence_after();
 }
 
-__global__ void __launch_bounds__(kUcThreads, 1)
-    k_uconv(const __grid_constant__ CUtensorMap tRBh, const __grid_constant__ CUtensorMap tRBl,
-            const __grid_constant__ CUtensorMap tXh, const __grid_constant__ CUtensorMap tXl,
-            const __grid_constant__ CUtensorMap tRAh, const __grid_constant__ CUtensorMap tRAl,
-            const __grid_constant__ CUtensorMap tRGAh, const __grid_constant__ CUtensorMap tRGAl,
-            const __grid_constant__ CUtensorMap tRGBh, const __grid_constant__ CUtensorMap tRGBl, UconvArgs a) {
+__device__ __forceinline__ void uconv_cta(const CUtensorMap *pRBh, const CUtensorMap *pRBl, const CUtensorMap *pXh, const CUtensorMap *pXl, const CUtensorMap *pRAh, const CUtensorMap *pRAl, const CUtensorMap *pRGAh, const CUtensorMap *pRGAl, const CUtensorMap *pRGBh, const CUtensorMap *pRGBl, const UconvArgs &a) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *sm = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ __align__(8) uint64_t bar_in0, bar_in1, bar_mma;
@@ -133,24 +128,24 @@ __global__ void __launch_bounds__(kUcThreads, 1)
     // constant tables first: they do not depend on the previous kernel
     mbar_arrive_expect_tx(&bar_in0, 65536 + kUcTwBytes);
     bulk_load(sm + kUcTw, a.twiddle, kUcTwBytes, &bar_in0);
-    tma_load_2d(sm + kUcRB, &tRBh, &bar_in0, 0, 0);
-    tma_load_2d(sm + kUcRB + 16384, &tRBl, &bar_in0, 0, 0);
+    tma_load_2d(sm + kUcRB, pRBh, &bar_in0, 0, 0);
+    tma_load_2d(sm + kUcRB + 16384, pRBl, &bar_in0, 0, 0);
     mbar_arrive_expect_tx(&bar_in1, 65536);
-    tma_load_2d(sm + kUcRA, &tRAh, &bar_in1, 0, 0);
-    tma_load_2d(sm + kUcRA + 8192, &tRAl, &bar_in1, 0, 0);
-    tma_load_2d(sm + kUcRGA, &tRGAh, &bar_in1, 0, 0);
-    tma_load_2d(sm + kUcRGA + 8192, &tRGAl, &bar_in1, 0, 0);
-    tma_load_2d(sm + kUcRGB, &tRGBh, &bar_in1, 0, 0);
-    tma_load_2d(sm + kUcRGB + 8192, &tRGBh, &bar_in1, 64, 0);
-    tma_load_2d(sm + kUcRGB + 16384, &tRGBl, &bar_in1, 0, 0);
-    tma_load_2d(sm + kUcRGB + 24576, &tRGBl, &bar_in1, 64, 0);
+    tma_load_2d(sm + kUcRA, pRAh, &bar_in1, 0, 0);
+    tma_load_2d(sm + kUcRA + 8192, pRAl, &bar_in1, 0, 0);
+    tma_load_2d(sm + kUcRGA, pRGAh, &bar_in1, 0, 0);
+    tma_load_2d(sm + kUcRGA + 8192, pRGAl, &bar_in1, 0, 0);
+    tma_load_2d(sm + kUcRGB, pRGBh, &bar_in1, 0, 0);
+    tma_load_2d(sm + kUcRGB + 8192, pRGBh, &bar_in1, 64, 0);
+    tma_load_2d(sm + kUcRGB + 16384, pRGBl, &bar_in1, 0, 0);
+    tma_load_2d(sm + kUcRGB + 24576, pRGBl, &bar_in1, 64, 0);
     // the phi spectrum is the previous kernel's output
     pdl_wait();
     const int x0 = blockIdx.x * (kUcModes * 32);
-    tma_load_2d(sm + kUcX, &tXh, &bar_in0, x0, 0);
-    tma_load_2d(sm + kUcX + 8192, &tXh, &bar_in0, x0 + 64, 0);
-    tma_load_2d(sm + kUcX + 16384, &tXl, &bar_in0, x0, 0);
-    tma_load_2d(sm + kUcX + 24576, &tXl, &bar_in0, x0 + 64, 0);
+    tma_load_2d(sm + kUcX, pXh, &bar_in0, x0, 0);
+    tma_load_2d(sm + kUcX + 8192, pXh, &bar_in0, x0 + 64, 0);
+    tma_load_2d(sm + kUcX + 16384, pXl, &bar_in0, x0, 0);
+    tma_load_2d(sm + kUcX + 24576, pXl, &bar_in0, x0 + 64, 0);
     // ---- S1: D1[(m, i1)][(p2, ro)] at TMEM columns 0..127 (the input slice is the A
     // operand, MN-major, so every TMEM lane is one (mode, i1) and its (re, im) pairs sit
     // in adjacent columns) ----
@@ -396,6 +391,40 @@ __global__ void __launch_bounds__(kUcThreads, 1)
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, kUcTmemCols);
+}
+
+__global__ void __launch_bounds__(kUcThreads, 1)
+    k_uconv(const __grid_constant__ CUtensorMap tRBh,
+    const __grid_constant__ CUtensorMap tRBl,
+    const __grid_constant__ CUtensorMap tXh,
+    const __grid_constant__ CUtensorMap tXl,
+    const __grid_constant__ CUtensorMap tRAh,
+    const __grid_constant__ CUtensorMap tRAl,
+    const __grid_constant__ CUtensorMap tRGAh,
+    const __grid_constant__ CUtensorMap tRGAl,
+    const __grid_constant__ CUtensorMap tRGBh,
+    const __grid_constant__ CUtensorMap tRGBl, UconvArgs a) {
+  uconv_cta(&tRBh, &tRBl, &tXh, &tXl, &tRAh, &tRAl, &tRGAh, &tRGAl, &tRGBh, &tRGBl, a);
+}
+
+// The same for a group of disks of one grid (batched sweeps): blockIdx.y is the disk; its
+// own operand maps sit with its arguments in a device array.
+struct __align__(64) UconvDisk {
+  CUtensorMap xh, xl;  // the disk's input slice Xin (hi / lo)
+  UconvArgs a;
+};
+
+__global__ void __launch_bounds__(kUcThreads, 1)
+    k_uconv_group(const __grid_constant__ CUtensorMap tRBh,
+    const __grid_constant__ CUtensorMap tRBl,
+    const __grid_constant__ CUtensorMap tRAh,
+    const __grid_constant__ CUtensorMap tRAl,
+    const __grid_constant__ CUtensorMap tRGAh,
+    const __grid_constant__ CUtensorMap tRGAl,
+    const __grid_constant__ CUtensorMap tRGBh,
+    const __grid_constant__ CUtensorMap tRGBl, const UconvDisk *__restrict__ disks) {
+  const UconvDisk &d = disks[blockIdx.y];
+  uconv_cta(&tRBh, &tRBl, &d.xh, &d.xl, &tRAh, &tRAl, &tRGAh, &tRGAl, &tRGBh, &tRGBl, d.a);
 }
 
 }  // namespace tc
