@@ -56,7 +56,7 @@ def propose(pred, X, taken, target, batch, min_dist):
     return chosen
 
 
-def steer(predict, hydro, target, tol, budget, batch=16, pool=4096, seed=777, grid=128, bound=0.05,
+def steer(predict, hydro, target, tol, budget, batch=16, pool=4096, seed=777, grid=256, bound=0.05,
           min_dist=0.05, refine=None):
     """Run at most `budget` hydro runs in rounds of `batch`, proposed by the surrogate.
 
@@ -95,14 +95,14 @@ def steer(predict, hydro, target, tol, budget, batch=16, pool=4096, seed=777, gr
             "hits": int(np.sum(np.abs(y_hydro - target) <= tol))}
 
 
-def uniform(hydro, target, tol, budget, seed=778, grid=128):
+def uniform(hydro, target, tol, budget, seed=778, grid=256):
     """The same budget spent on a uniform draw of the sweep law."""
     pts = S.draw(budget, seed=seed, grids=(grid,))
     y = np.asarray(hydro(pts), dtype=np.float64)
     return {"points": pts, "gamma_hydro": y, "hits": int(np.sum(np.abs(y - target) <= tol))}
 
 
-def hydro_gamma(points, tlim=12.0, dtout=0.25, device=-1):
+def hydro_gamma(points, tlim=16.0, dtout=0.25, device=-1):
     """gamma of each sweep point from the batched mixed-precision hydro: the linear phase
     of its m = 2 records (t >= 1 until |C2|/|C0| > 0.05), NaN where no fit is possible."""
     from . import Batch

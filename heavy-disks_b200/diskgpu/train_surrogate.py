@@ -1,6 +1,9 @@
 """Build the surrogate's training set from batched hydro runs and train it on the GPU.
 
-  python -m diskgpu.train_surrogate --runs 512 --grid 128 --tlim 16 --out <dir>
+  python -m diskgpu.train_surrogate --runs 4096 --grid 256 --tlim 16 --batch 1024 --out <dir>
+
+(the defaults: 4096 sweep-law runs at 256^2 to t = 16, the set the shipped network in
+diskgpu/data was trained on; about ten minutes of batched hydro on one B200).
 
 Draws sweep points with the sweep law (diskgpu.sweep.draw, fixed seed), runs them in
 batches of disks advanced together (dg_batch, mixed precision; same-grid disks step as one
@@ -55,10 +58,10 @@ def run_points(pts, tlim, batch=128, dtout=0.25):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--runs", type=int, default=512)
-    ap.add_argument("--grid", type=int, default=128)
+    ap.add_argument("--runs", type=int, default=4096)
+    ap.add_argument("--grid", type=int, default=256)
     ap.add_argument("--tlim", type=float, default=16.0)
-    ap.add_argument("--batch", type=int, default=128)
+    ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--seed", type=int, default=12345)
     ap.add_argument("--epochs", type=int, default=400)
     ap.add_argument("--out", default=".")

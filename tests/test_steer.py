@@ -59,7 +59,8 @@ def test_proposals_are_spread_and_unique():
 
 @pytest.mark.gpu
 def test_steered_hydro_sweep_beats_uniform_draw():
-    """The shipped surrogate steers 48 hydro runs (128^2, mixed precision, t = 12) at the
+    """The shipped surrogate steers 48 hydro runs (256^2, mixed precision, t = 16: the grid
+    and time of its training set) at the
     contour gamma = 0.5 +- 0.05; the same budget drawn uniformly from the sweep law lands
     fewer runs on it.  The hydro judges every proposal (the network's error is recorded)."""
     from diskgpu.surrogate import TRAINED, Surrogate

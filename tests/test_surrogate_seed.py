@@ -46,11 +46,12 @@ def test_shipped_surrogate_beats_constant_guess_on_held_out_runs():
     Xtr, Ytr, Xho, Yho = X[:-n_hold], Y[:-n_hold], X[-n_hold:], Y[-n_hold:]
     mae = np.abs(_predict(d, Xho) - Yho).mean(axis=0)
     mae_const = np.abs(Ytr.mean(axis=0) - Yho).mean(axis=0)
-    # gamma and the saturated ratio: over 10x better than the constant guess.  Omega_p varies
-    # little over the sweep (its spread, ~0.06, is close to the fit noise of 128^2 runs), so
-    # the network can only beat the constant by a margin there.
+    # gamma and the saturated ratio: over 10x better than the constant guess (about 30x and
+    # 20x for the shipped network).  Omega_p varies little over the sweep (mean deviation
+    # ~0.027, of the order of the fit noise of 256^2 runs to t = 16), so the margin is
+    # smaller there (about 3x).
     assert mae[0] <= 0.1 * mae_const[0] and mae[2] <= 0.1 * mae_const[2], (mae, mae_const)
-    assert mae[1] <= 0.85 * mae_const[1], (mae, mae_const)
+    assert mae[1] <= 0.5 * mae_const[1], (mae, mae_const)
     # and the same figures the training run reported (GPU network vs FP64 oracle evaluation)
     rep = d["report"]["mae_held_out"]
     np.testing.assert_allclose(mae, [rep["gamma"], rep["omega_p"], rep["sat_ratio"]], rtol=0.05)
