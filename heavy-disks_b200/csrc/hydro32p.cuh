@@ -1,7 +1,16 @@
-// Packed form of the tiled mixed-precision hydro step: the same stages, shared-memory plan
-// and arithmetic as hydro32t.cuh, with every thread advancing two adjacent columns at once
-// in FP32x2 registers (Blackwell's paired FADD2 / FMUL2 / FFMA2), so one instruction, one
-// shared-memory access and one set of row constants serve two zones.
+// Packed form of the tiled mixed-precision hydro step: the arithmetic of hydro32t.cuh, with
+// every thread advancing two adjacent columns at once in FP32x2 registers (Blackwell's
+// paired FADD2 / FMUL2 / FFMA2), so one instruction, one shared-memory access and one set
+// of row constants serve two zones.
+//
+// Stages, one warp per row (CTA barriers only where a stage reads other warps' rows):
+//   S0 stage sigma, u, w, dPhi of rows i0-3 .. i0+kTileI+2        | barrier
+//   S1 pressure perturbation of the staged rows                     | barrier
+//   S2 source kick of rows i0-2 .. i0+kTileI+1 (hydro.hpp:73-96)    | barrier
+//   S3 radial faces i0 .. i0+kTileI-1, two rows per warp            | barrier
+//   S4-S6 per output row, in registers: the row's radial gather, its azimuthal faces
+//      (neighbours by lane shuffles) and azimuthal gather, outputs and CFL rate; the warp
+//      of the last row first computes the tile's top face i0+kTileI.
 //
 // Tile: kTileI rows x kTileJp = 58 output columns.  Stored columns c in [0, 64) hold the
 // unwrapped columns J = j0 - 3 + c (a 3-column halo on each side); the outputs are
@@ -31,7 +40,8 @@ constexpr int kLdP = kLd32t + 4;           // floats per staged row: a TMA box f
 constexpr int kWarps32p = kThreads32t / 32;  // 8 row groups, one warp each
 constexpr int kItLoadP = (kRows32t + kWarps32p - 1) / kWarps32p;
 constexpr int kItSrcP = (kSrcRows32t + kWarps32p - 1) / kWarps32p;
-constexpr int kItFaceP = (kFaceRows32t + kWarps32p - 1) / kWarps32p;
+constexpr int kItFaceP = kTileI / kWarps32p;  // S3 face rows per warp (the last face is S4's)
+static_assert(kItFaceP * kWarps32p == kTileI, "face rows split evenly over the warps");
 constexpr int kItOutP = (kTileI + kWarps32p - 1) / kWarps32p;
 static_assert(kItOutP * kWarps32p == kTileI, "output rows split evenly over the warps");
 // shared-memory plan of this kernel in floats: the five staged fields first (each one TMA
@@ -109,9 +119,7 @@ __device__ __forceinline__ void hydro32p_tile(
   F2 *U1 = U0 + L2, *W1 = W0 + L2;  // source row rs = stored row rs + 1
   F2 *FF = reinterpret_cast<F2 *>(sm32t + kOffFP), *FR = FF + kFaceArr32t / 2, *GA = FR + kFaceArr32t / 2,
      *GB = GA + kFaceArr32t / 2;
-  F2 *U2 = DP, *W2 = PH;            // S4 outputs over the dead source inputs
-  F2 *PF = FF, *PR = FR, *PG = GA;  // S5 outputs over the dead radial fluxes
-  F2 *S3 = U1;                      // new sigma for the mode sums
+  F2 *S3 = DP;  // new sigma for the mode sums, over the pressure perturbation (dead after S2)
 
   const int iend = (i0 + kTileI < Nu) ? i0 + kTileI : Nu;
   const int jc = wrap_col(xs0 + 2 * lane, Nphi);  // global column of this lane's first element (even)
@@ -300,133 +308,125 @@ __device__ __forceinline__ void hydro32p_tile(
   }
   __syncthreads();
 
-  // ---- S3: radial faces f = i0 .. i0+kTileI (hydro.hpp:107-130) ----
-#pragma unroll
-  for (int k = 0; k < kItFaceP; ++k) {
-    const int fr = wp + kWarps32p * k, f = i0 + fr;
-    if (fr < kFaceRows32t) {
-      F2 F = S(0.f), FRv = S(0.f), GAv = S(0.f), GBv = S(0.f);
-      if (IN || (f >= 1 && f <= Nu - 1)) {
-        const int xs = (f - 2 - ib) * L2 + lane;  // sigma rows f-2 .. f+1
-        const int xu = (f - 3 - ib) * L2 + lane;  // u1 / w1 rows f-2 .. f+1
-        const F2 s0 = SG[xs], s1 = SG[xs + L2], s2 = SG[xs + 2 * L2], s3 = SG[xs + 3 * L2];
-        const F2 u0 = U1[xu], u1 = U1[xu + L2], u2 = U1[xu + 2 * L2], u3 = U1[xu + 3 * L2];
-        const F2 w0 = W1[xu], w1 = W1[xu + L2], w2 = W1[xu + 2 * L2], w3 = W1[xu + 3 * L2];
-        const F2 vf = mul(S(0.5f), add(u1, u2));
-        const bool ux = vf.x > 0.f, uy = vf.y > 0.f;
-        const F2 vdt = mul(vf, S(dt));
-        // face constants: DS0 / DV of faces f-1, f, f+1; Af, invdRl, invdRr of face f
-        const float4 cm = RC4(3, f - 1), cf = RC4(3, f), cp = RC4(3, f + 1), ca = RC4(4, f);
-        const F2 hu = mul(S(0.5f), sub(S(1.f), mul(vdt, S(ca.y))));
-        const F2 hd = mul(S(-0.5f), add(S(1.f), mul(vdt, S(ca.z))));
-        const F2 hf = sel(ux, uy, hu, hd);
-        // cells cc-1, cc, cc+1 with cc = f-1 (upwind from below) or f
-        const F2 sa = sel(ux, uy, s0, s1), sb = sel(ux, uy, s1, s2), sc = sel(ux, uy, s2, s3);
-        const F2 ua = sel(ux, uy, u0, u1), ub = sel(ux, uy, u1, u2), uc = sel(ux, uy, u2, u3);
-        const F2 wa = sel(ux, uy, w0, w1), wb = sel(ux, uy, w1, w2), wc = sel(ux, uy, w2, w3);
-        const F2 ds_c = sels(ux, uy, cm.z, cf.z), ds_c1 = sels(ux, uy, cf.z, cp.z);
-        const F2 dv_c = sels(ux, uy, cm.w, cf.w), dv_c1 = sels(ux, uy, cf.w, cp.w);
-        const F2 s0_c = sels(ux, uy, RC(tS0, f - 1), RC(tS0, f));
-        F2 kS = vanleer(add(ds_c1, sub(sc, sb)), add(ds_c, sub(sb, sa)));
-        F2 kU = vanleer(sub(uc, ub), sub(ub, ua));
-        F2 kV = vanleer(add(dv_c1, sub(wc, wb)), add(dv_c, sub(wb, wa)));
-        if (!IN) {  // no slope in the first and last cell (hydro.hpp:117-119)
-          const int ccx = ux ? f - 1 : f, ccy = uy ? f - 1 : f;
-          const bool okx = ccx > 0 && ccx < Nu - 1, oky = ccy > 0 && ccy < Nu - 1;
-          kS = sel(okx, oky, kS, S(0.f));
-          kU = sel(okx, oky, kU, S(0.f));
-          kV = sel(okx, oky, kV, S(0.f));
-        }
-        const F2 Sf = fma(hf, kS, add(s0_c, sb));
-        const F2 uf = fma(hf, kU, ub);
-        const float dVf = cf.w;
-        const F2 Df = fma(hf, kV, add(sels(ux, uy, 0.f, dVf), wb));  // vphi_f - V0(f-1)
-        F = mul(mul(vf, Sf), S(ca.x));
-        FRv = mul(F, uf);
-        GAv = mul(F, Df);
-        GBv = mul(F, sub(Df, S(dVf)));
+  // radial face f (hydro.hpp:107-130): mass flux F, and the fluxes of u and of vphi seen
+  // from the rows below (GA) and above (GB) the face
+  struct Face { F2 F, FR, GA, GB; };
+  auto radial_face = [&](int f) -> Face {
+    F2 F = S(0.f), FRv = S(0.f), GAv = S(0.f), GBv = S(0.f);
+    if (IN || (f >= 1 && f <= Nu - 1)) {
+      const int xs = (f - 2 - ib) * L2 + lane;  // sigma rows f-2 .. f+1
+      const int xu = (f - 3 - ib) * L2 + lane;  // u1 / w1 rows f-2 .. f+1
+      const F2 s0 = SG[xs], s1 = SG[xs + L2], s2 = SG[xs + 2 * L2], s3 = SG[xs + 3 * L2];
+      const F2 u0 = U1[xu], u1 = U1[xu + L2], u2 = U1[xu + 2 * L2], u3 = U1[xu + 3 * L2];
+      const F2 w0 = W1[xu], w1 = W1[xu + L2], w2 = W1[xu + 2 * L2], w3 = W1[xu + 3 * L2];
+      const F2 vf = mul(S(0.5f), add(u1, u2));
+      const bool ux = vf.x > 0.f, uy = vf.y > 0.f;
+      const F2 vdt = mul(vf, S(dt));
+      // face constants: DS0 / DV of faces f-1, f, f+1; Af, invdRl, invdRr of face f
+      const float4 cm = RC4(3, f - 1), cf = RC4(3, f), cp = RC4(3, f + 1), ca = RC4(4, f);
+      const F2 hu = mul(S(0.5f), sub(S(1.f), mul(vdt, S(ca.y))));
+      const F2 hd = mul(S(-0.5f), add(S(1.f), mul(vdt, S(ca.z))));
+      const F2 hf = sel(ux, uy, hu, hd);
+      // cells cc-1, cc, cc+1 with cc = f-1 (upwind from below) or f
+      const F2 sa = sel(ux, uy, s0, s1), sb = sel(ux, uy, s1, s2), sc = sel(ux, uy, s2, s3);
+      const F2 ua = sel(ux, uy, u0, u1), ub = sel(ux, uy, u1, u2), uc = sel(ux, uy, u2, u3);
+      const F2 wa = sel(ux, uy, w0, w1), wb = sel(ux, uy, w1, w2), wc = sel(ux, uy, w2, w3);
+      const F2 ds_c = sels(ux, uy, cm.z, cf.z), ds_c1 = sels(ux, uy, cf.z, cp.z);
+      const F2 dv_c = sels(ux, uy, cm.w, cf.w), dv_c1 = sels(ux, uy, cf.w, cp.w);
+      const F2 s0_c = sels(ux, uy, RC(tS0, f - 1), RC(tS0, f));
+      F2 kS = vanleer(add(ds_c1, sub(sc, sb)), add(ds_c, sub(sb, sa)));
+      F2 kU = vanleer(sub(uc, ub), sub(ub, ua));
+      F2 kV = vanleer(add(dv_c1, sub(wc, wb)), add(dv_c, sub(wb, wa)));
+      if (!IN) {  // no slope in the first and last cell (hydro.hpp:117-119)
+        const int ccx = ux ? f - 1 : f, ccy = uy ? f - 1 : f;
+        const bool okx = ccx > 0 && ccx < Nu - 1, oky = ccy > 0 && ccy < Nu - 1;
+        kS = sel(okx, oky, kS, S(0.f));
+        kU = sel(okx, oky, kU, S(0.f));
+        kV = sel(okx, oky, kV, S(0.f));
       }
-      const int x = fr * LF + lane;
-      FF[x] = F; FR[x] = FRv; GA[x] = GAv; GB[x] = GBv;
+      const F2 Sf = fma(hf, kS, add(s0_c, sb));
+      const F2 uf = fma(hf, kU, ub);
+      const float dVf = cf.w;
+      const F2 Df = fma(hf, kV, add(sels(ux, uy, 0.f, dVf), wb));  // vphi_f - V0(f-1)
+      F = mul(mul(vf, Sf), S(ca.x));
+      FRv = mul(F, uf);
+      GAv = mul(F, Df);
+      GBv = mul(F, sub(Df, S(dVf)));
     }
-  }
-  __syncthreads();
+    return Face{F, FRv, GAv, GBv};
+  };
 
-  // ---- S4: radial gather of rows i0 .. iend-1 (hydro.hpp:131-139), in place ----
+  auto store_face = [&](int fr) {
+    const Face fc = radial_face(i0 + fr);
+    const int x = fr * LF + lane;
+    FF[x] = fc.F; FR[x] = fc.FR; GA[x] = fc.GA; GB[x] = fc.GB;
+  };
+  // ---- S3: radial faces f = i0 .. i0+kTileI-1, two face rows per warp.  The last face,
+  // i0+kTileI, is needed only by row i0+kTileI-1: the warp that gathers that row computes
+  // it after the barrier, while the other warps go on (each lane reads back only its own
+  // entries, so no further synchronisation is needed). ----
+#pragma unroll
+  for (int k = 0; k < kItFaceP; ++k) store_face(wp + kWarps32p * k);
+  __syncthreads();
+  if (wp == (kTileI - 1) % kWarps32p) store_face(kTileI);
+
+  // ---- S4-S6, one output row per warp iteration: radial gather (hydro.hpp:131-139),
+  // azimuthal faces 2l and 2l+1 (the left faces of the lane's columns; hydro.hpp:150-170),
+  // azimuthal gather, floor (hydro.hpp:69), outputs and CFL rate.  A row's three stages read
+  // only that row (neighbour columns by lane shuffles) and the radial fluxes of S3, so they
+  // run back to back in registers with no CTA barrier between them. ----
 #pragma unroll
   for (int k = 0; k < kItOutP; ++k) {
     const int ri = wp + kWarps32p * k, i = i0 + ri;
-    if (IN || i < iend) {
+    if (IN || i < iend) {  // warp-uniform: every lane takes part in the shuffles below
       const int xs = (i - ib) * L2 + lane, xu = (i - ib - 1) * L2 + lane, xf = ri * LF + lane;
+      const float4 c0 = RC4(0, i), c2 = RC4(2, i);  // S0 invS0 V0 a0 | invVol invdl Aphi R32
+      const float S0 = c0.x, V = c0.z, iv = c2.x, idl = c2.y, A = c2.z;
+      // S4: radial gather
       const F2 sgi = SG[xs], u1i = U1[xu], w1i = W1[xu];
-      const float S0 = RC(tS0, i), iv = RC(tInvVol, i);
       const F2 s = add(S(S0), sgi);
       const F2 s2 = fma(mul(S(dt), sub(FF[xf], FF[xf + LF])), S(iv), sgi);
       const F2 sn = add(S(S0), s2);
-      const F2 d = make_float2(sn.x < 1e-10f ? 1e-10f : sn.x, sn.y < 1e-10f ? 1e-10f : sn.y);
-      const F2 rd = rcp(d);
-      const F2 u2 = mul(fma(mul(S(dt), sub(FR[xf], FR[xf + LF])), S(iv), mul(s, u1i)), rd);
-      const F2 w2 = mul(fma(mul(S(dt), sub(GB[xf], GA[xf + LF])), S(iv), mul(s, w1i)), rd);
-      SG[xs] = s2;
-      U2[xs] = u2;
-      W2[xs] = w2;
-    }
-  }
-  __syncthreads();
-
-  // ---- S5: azimuthal faces 2l and 2l+1 (left faces of those columns; hydro.hpp:150-170) ----
-#pragma unroll
-  for (int k = 0; k < kItOutP; ++k) {
-    const int ri = wp + kWarps32p * k, i = i0 + ri;
-    if (IN || i < iend) {
-      const int x = (i - ib) * L2 + lane;
-      const F2 sm = SG[x], um = U2[x], wm = W2[x];
-      // columns 2l-2, 2l-1 from the left lane, 2l+2 from the right lane
-      const float sL0 = up1(sm.x), sL1 = up1(sm.y), sR = dn1(sm.x);
-      const float uL0 = up1(um.x), uL1 = up1(um.y), uR = dn1(um.x);
-      const float wL0 = up1(wm.x), wL1 = up1(wm.y), wR = dn1(wm.x);
-      const float4 c0 = RC4(0, i), c2 = RC4(2, i);  // S0 invS0 V0 a0 | invVol invdl Aphi R32
-      const float V = c0.z, idl = c2.y, S0 = c0.x, A = c2.z;
-      const F2 dv = mul(S(0.5f), add(make_float2(wL1, wm.x), make_float2(wm.x, wm.y)));
-      const F2 vf = add(S(V), dv);
-      const bool ux = vf.x > 0.f, uy = vf.y > 0.f;
-      const F2 vdt = mul(mul(vf, S(dt)), S(idl));
-      const F2 hf = sel(ux, uy, mul(S(0.5f), sub(S(1.f), vdt)), mul(S(-0.5f), add(S(1.f), vdt)));
-      // face 2l: cells (2l-2, 2l-1, 2l) upwind from the left, else (2l-1, 2l, 2l+1);
-      // face 2l+1: (2l-1, 2l, 2l+1) or (2l, 2l+1, 2l+2)
-      const F2 sa = make_float2(ux ? sL0 : sL1, uy ? sL1 : sm.x), sb = make_float2(ux ? sL1 : sm.x, uy ? sm.x : sm.y),
-               sc = make_float2(ux ? sm.x : sm.y, uy ? sm.y : sR);
-      const F2 ua = make_float2(ux ? uL0 : uL1, uy ? uL1 : um.x), ub = make_float2(ux ? uL1 : um.x, uy ? um.x : um.y),
-               uc = make_float2(ux ? um.x : um.y, uy ? um.y : uR);
-      const F2 wa = make_float2(ux ? wL0 : wL1, uy ? wL1 : wm.x), wb = make_float2(ux ? wL1 : wm.x, uy ? wm.x : wm.y),
-               wc = make_float2(ux ? wm.x : wm.y, uy ? wm.y : wR);
-      const F2 sf = fma(hf, vanleer(sub(sc, sb), sub(sb, sa)), sb);
-      const F2 Sf = add(S(S0), sf);
-      const F2 uf = fma(hf, vanleer(sub(uc, ub), sub(ub, ua)), ub);
-      const F2 wf = fma(hf, vanleer(sub(wc, wb), sub(wb, wa)), wb);
-      const F2 Ffull = mul(mul(vf, Sf), S(A));
-      const int xf = ri * LF + lane;
-      PF[xf] = mul(S(A), fma(S(V), sf, mul(dv, Sf)));
-      PR[xf] = mul(Ffull, uf);
-      PG[xf] = mul(Ffull, wf);
-    }
-  }
-  __syncthreads();
-
-  // ---- S6: azimuthal gather, floor (hydro.hpp:69), outputs, CFL rate ----
-#pragma unroll
-  for (int k = 0; k < kItOutP; ++k) {
-    const int ri = wp + kWarps32p * k, i = i0 + ri;
-    if (IN || i < iend) {
-      const int x = (i - ib) * L2 + lane, xf = ri * LF + lane;
-      const F2 fm = PF[xf], fr = PR[xf], fg = PG[xf];
-      // right face of column 2l+1 is the right lane's first face
+      const F2 dd = make_float2(sn.x < 1e-10f ? 1e-10f : sn.x, sn.y < 1e-10f ? 1e-10f : sn.y);
+      const F2 rdd = rcp(dd);
+      const F2 u2 = mul(fma(mul(S(dt), sub(FR[xf], FR[xf + LF])), S(iv), mul(s, u1i)), rdd);
+      const F2 w2 = mul(fma(mul(S(dt), sub(GB[xf], GA[xf + LF])), S(iv), mul(s, w1i)), rdd);
+      // S5: azimuthal faces; columns 2l-2, 2l-1 from the left lane, 2l+2 from the right lane
+      F2 fm, fr, fg;
+      {
+        const F2 sm = s2, um = u2, wm = w2;
+        const float sL0 = up1(sm.x), sL1 = up1(sm.y), sR = dn1(sm.x);
+        const float uL0 = up1(um.x), uL1 = up1(um.y), uR = dn1(um.x);
+        const float wL0 = up1(wm.x), wL1 = up1(wm.y), wR = dn1(wm.x);
+        const F2 dv = mul(S(0.5f), add(make_float2(wL1, wm.x), make_float2(wm.x, wm.y)));
+        const F2 vf = add(S(V), dv);
+        const bool ux = vf.x > 0.f, uy = vf.y > 0.f;
+        const F2 vdt = mul(mul(vf, S(dt)), S(idl));
+        const F2 hf = sel(ux, uy, mul(S(0.5f), sub(S(1.f), vdt)), mul(S(-0.5f), add(S(1.f), vdt)));
+        // face 2l: cells (2l-2, 2l-1, 2l) upwind from the left, else (2l-1, 2l, 2l+1);
+        // face 2l+1: (2l-1, 2l, 2l+1) or (2l, 2l+1, 2l+2)
+        const F2 sa = make_float2(ux ? sL0 : sL1, uy ? sL1 : sm.x),
+                 sb = make_float2(ux ? sL1 : sm.x, uy ? sm.x : sm.y),
+                 sc = make_float2(ux ? sm.x : sm.y, uy ? sm.y : sR);
+        const F2 ua = make_float2(ux ? uL0 : uL1, uy ? uL1 : um.x),
+                 ub = make_float2(ux ? uL1 : um.x, uy ? um.x : um.y),
+                 uc = make_float2(ux ? um.x : um.y, uy ? um.y : uR);
+        const F2 wa = make_float2(ux ? wL0 : wL1, uy ? wL1 : wm.x),
+                 wb = make_float2(ux ? wL1 : wm.x, uy ? wm.x : wm.y),
+                 wc = make_float2(ux ? wm.x : wm.y, uy ? wm.y : wR);
+        const F2 sf = fma(hf, vanleer(sub(sc, sb), sub(sb, sa)), sb);
+        const F2 Sf = add(S(S0), sf);
+        const F2 uf = fma(hf, vanleer(sub(uc, ub), sub(ub, ua)), ub);
+        const F2 wf = fma(hf, vanleer(sub(wc, wb), sub(wb, wa)), wb);
+        const F2 Ffull = mul(mul(vf, Sf), S(A));
+        fm = mul(S(A), fma(S(V), sf, mul(dv, Sf)));
+        fr = mul(Ffull, uf);
+        fg = mul(Ffull, wf);
+      }
+      // S6: azimuthal gather; the right face of column 2l+1 is the right lane's first face
       const F2 fm1 = make_float2(fm.y, dn1(fm.x)), fr1 = make_float2(fr.y, dn1(fr.x)), fg1 = make_float2(fg.y, dn1(fg.x));
       if (outx || outy) {
-        const float4 c0 = RC4(0, i), c2 = RC4(2, i);  // S0 invS0 V0 a0 | invVol invdl Aphi R32
-        const float iv = c2.x, S0 = c0.x;
-        const F2 s2 = SG[x], u2 = U2[x], w2 = W2[x];
-        const F2 sn2 = add(S(S0), s2);
+        const F2 sn2 = sn;
         F2 s3 = fma(mul(S(dt), sub(fm, fm1)), S(iv), s2);
         const F2 sn3 = add(S(S0), s3);
         const bool flx = sn3.x < 1e-10f, fly = sn3.y < 1e-10f;
@@ -463,7 +463,7 @@ __device__ __forceinline__ void hydro32p_tile(
         const F2 cs = G2 ? make_float2(sqrt_pos(gk * scl.x), sqrt_pos(gk * scl.y))
                          : make_float2(sqrt_pos(gk * powf(scl.x, g.gamma - 1.f)),
                                        sqrt_pos(gk * powf(scl.y, g.gamma - 1.f)));
-        const float V = c0.z, idR = RC(tInvdR, i), idl = c2.y;
+        const float idR = RC(tInvdR, i);
         const F2 rate = fma(add(make_float2(fabsf(V + w3.x), fabsf(V + w3.y)), cs), S(idl),
                             mul(add(make_float2(fabsf(u3.x), fabsf(u3.y)), cs), S(idR)));
         if (outx) {

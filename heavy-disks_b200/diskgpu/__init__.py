@@ -258,15 +258,22 @@ def read_params(path, max_disks=1 << 16):
 class Disk:
     """One disk on one GPU: the handle of include/diskgpu.h."""
 
-    def __init__(self, Nu=128, Nphi=128, eps=0.02, selfgrav=1, amp=1e-3, precision="fp64", params=None, **kw):
+    def __init__(self, Nu=128, Nphi=128, eps=0.02, selfgrav=1, amp=None, precision="fp64", params=None, **kw):
+        """With `params` (a Params), the disk takes them with Nu, Nphi, precision and any
+        keyword given here replacing theirs (amp only when given); otherwise the standard
+        disk of default_params with these values (amp 1e-3 unless given)."""
         if params is not None:
             self.p = Params.from_buffer_copy(params)
-            for k, v in dict(Nu=Nu, Nphi=Nphi, precision=precision, amp=amp, **kw).items():
+            over = dict(Nu=Nu, Nphi=Nphi, precision=precision, **kw)
+            if amp is not None:
+                over["amp"] = amp
+            for k, v in over.items():
                 if k == "precision" and isinstance(v, str):
                     v = {"fp64": FP64, "mixed": MIXED}[v]
                 setattr(self.p, k, v)
         else:
-            self.p = default_params(Nu=Nu, Nphi=Nphi, eps=eps, selfgrav=selfgrav, amp=amp, precision=precision, **kw)
+            self.p = default_params(Nu=Nu, Nphi=Nphi, eps=eps, selfgrav=selfgrav, amp=1e-3 if amp is None else amp,
+                                    precision=precision, **kw)
         self.Nu, self.Nphi = Nu, Nphi
         h = C.c_void_p()
         rc = lib().dg_create(C.byref(self.p), C.byref(h))
