@@ -18,7 +18,8 @@ line also carries `fp64_same_disk` (the plain FP64 path on the same disk, timed 
 same K steps, and the mixed/FP64 ratio the metric names), `cufft_gravity` (the same padded
 convolution through cuFFT, as a timing comparison only) and `batched_sweep` (256 disks of
 the sweep law, grids 128^2..512^2, advanced together by dg_batch; inside it `batched_1024`,
-16 sweep-law disks all at 1024^2, and their ratio to the plain FP64 path at 1024^2).
+16 sweep-law disks all at 1024^2 as one graph branch each (with the grouped kernels'
+figure beside it), and their ratio to the plain FP64 path at 1024^2).
 
 --impl reference times the reference's own CPU implementation (diskfft/src hydro.hpp +
 kalnajs.hpp compiled unmodified against the FFTW-API shim, with the reference Makefile's
@@ -424,7 +425,7 @@ def batched_sweep(a, device, grouped=True, ndisks=None, grids=None, tlim=None):
     import torch
     import diskgpu as D
     from diskgpu import sweep as S
-    os.environ["DISKGPU_BATCH_GROUPS"] = "1" if grouped else "0"
+    os.environ["DISKGPU_BATCH_GROUPS"] = "all" if grouped else "0"
     grid_list = grids or tuple(int(g) for g in a.batch_grids.split(","))
     tlim = a.batch_tlim if tlim is None else tlim
     pts = S.draw(ndisks or a.batch_disks, seed=a.batch_seed, grids=grid_list)
@@ -669,10 +670,11 @@ def main():
             batch = batched_sweep(a, local, grouped=True)
             batch["ungrouped"] = batched_sweep(a, local, grouped=False)["value"]
         if a.batch1024_disks > 0:
-            b1k = batched_sweep(a, local, grouped=True, ndisks=a.batch1024_disks, grids=(1024,),
+            # the default: one graph branch per 1024^2 disk; beside it the grouped kernels
+            b1k = batched_sweep(a, local, grouped=False, ndisks=a.batch1024_disks, grids=(1024,),
                                 tlim=a.batch1024_tlim)
-            b1k["ungrouped"] = batched_sweep(a, local, grouped=False, ndisks=a.batch1024_disks, grids=(1024,),
-                                             tlim=a.batch1024_tlim)["value"]
+            b1k["grouped_value"] = batched_sweep(a, local, grouped=True, ndisks=a.batch1024_disks, grids=(1024,),
+                                                 tlim=a.batch1024_tlim)["value"]
             if fp64 is not None and N == 1024:
                 b1k["over_fp64_plain_1024"] = b1k["value"] / fp64["value"]
             batch = dict(batch or {}, batched_1024=b1k)

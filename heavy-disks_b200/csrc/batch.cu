@@ -8,7 +8,12 @@
 // device-resident dt, time and record ring (dg::Ctl); a disk that reaches tlim turns the
 // rest of its launches into pass-throughs.  Branches whose disks have a smaller dt get
 // proportionally more steps per launch so that the branches finish together.
-// DISKGPU_BATCH_GROUPS=0 in the environment turns grouping off (every disk its own branch).
+// Grouping covers the dense-product grids by default.  1024^2 disks step as one branch
+// each unless DISKGPU_BATCH_GROUPS=all: their lone step already fills the GPU, and
+// separate branches overlap one disk's transforms with another's hydro and keep each
+// disk's row-tile hand-over, which measured faster than the grouped kernels (2.05e10
+// against 1.93e10 zone-updates/s for 16 disks).  DISKGPU_BATCH_GROUPS=0 turns grouping
+// off (every disk its own branch).
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -158,9 +163,10 @@ int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int ste
     {
       const char *ge = getenv("DISKGPU_BATCH_GROUPS");
       const bool grouping = !(ge && strcmp(ge, "0") == 0);
+      const bool group_fused = ge && strcmp(ge, "all") == 0;
       std::map<std::string, std::vector<int>> by_key;
       for (int k = 0; k < n; ++k) {
-        std::string key = grouping ? mixed_group_key(b->disks[k]) : std::string();
+        std::string key = grouping ? mixed_group_key(b->disks[k], group_fused) : std::string();
         if (key.empty()) {
           branches.emplace_back(1, k);
           continue;

@@ -10,9 +10,10 @@
 struct MixedState;  // mixed.cu
 struct MixedGroup;  // mixed.cu: disks of a batched sweep stepped by one launch per kernel
 struct dg_handle;
-// Grouping key of a disk ("" when it cannot join a group), group set-up, one step of the
-// whole group on a stream, and release.
-std::string mixed_group_key(const dg_handle *h);
+// Grouping key of a disk ("" when it cannot join a group; 1024^2 disks, whose fused
+// transforms have group forms, only with with_fused), group set-up, one step of the whole
+// group on a stream, and release.
+std::string mixed_group_key(const dg_handle *h, bool with_fused = true);
 MixedGroup *mixed_group_create(const std::vector<dg_handle *> &disks, std::string *err);
 int mixed_group_enqueue_step(MixedGroup *g, cudaStream_t st);
 void mixed_group_destroy(MixedGroup *g);

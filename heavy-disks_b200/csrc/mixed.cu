@@ -71,7 +71,8 @@ struct MixedState {
   enum HydroKind : int { kHydroWarp = 0, kHydroTile = 1, kHydroPacked = 2 };
   int hydro_kind = kHydroTile;
   // pipeline stages of each gravity product (slots: 0 phi DFT, 1-4 the u passes, 5 inverse
-  // phi DFT; 0 = chosen by K) and the tuner's record (autotune below)
+  // phi DFT; 0 = chosen by K, kPersist = the persistent kernel) and the tuner's record
+  // (autotune below)
   int ns[6] = {0, 0, 0, 0, 0, 0};
   // FP32 field tiles of the packed hydro kernel: sigma, u, w of both ping-pong buffers, dPhi
   CUtensorMap mSig[2], mU[2], mW[2], mPhi;
@@ -588,13 +589,38 @@ static cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, siz
   return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
-// gemm(): one split-BF16 product.  ns = pipeline stages (1, 2 or 4); 0 picks by K.
+// a product slot's "stages" value that selects the persistent GEMM (tc_gemm.cuh)
+constexpr int kPersist = 8;
+
+// SMs of the current device (the persistent products' grid)
+static int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      n <= 0)
+    n = 148;
+  return n;
+}
+
+// gemm(): one split-BF16 product.  ns = pipeline stages of the tile kernel (1, 2 or 4; 0
+// picks by K), or kPersist for the persistent kernel.
 template <int MODE, bool A_MN = false, bool B_MN = false>
 static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUtensorMap &Bh, const CUtensorMap &Bl,
                         int M, int N, int K, const tc::GemmArgs &base, cudaStream_t st, int ns = 0) {
   tc::GemmArgs a = base;
   a.M = M; a.N = N; a.K = K;
   if (M % tc::BM || N % tc::BN || K % tc::BK) return cudaErrorInvalidValue;
+  if (ns == kPersist) {
+    // the persistent warp-specialised kernel: one CTA per SM walks 128 x 128 tiles, the
+    // epilogue of one tile overlapping the loads and MMAs of the next
+    if (N % tc::BN2 == 0) {
+      tc::GemmDisk b;
+      b.hi = Bh; b.lo = Bl; b.args = a;
+      const int tn = N / tc::BN2, tm = M / tc::BM, nt = tn * tm, nsm = sm_count();
+      return launch_pdl(tc::k_gemm_persist<MODE, A_MN, B_MN>, dim3(nt < nsm ? nt : nsm), dim3(tc::kThreadsP),
+                        tc::kSmemP, st, Ah, Al, b, tn, tm, nt);
+    }
+    ns = 0;  // N not a multiple of 128: the tile kernel, stages by K
+  }
   dim3 grid(N / tc::BN, M / tc::BM);
   // short contractions (one or two K chunks) need no deep pipeline: fewer stages let more
   // CTAs share an SM and hide each tile's load / epilogue latency
@@ -614,6 +640,8 @@ static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUte
 template <int MODE, bool A_MN, bool B_MN>
 static cudaError_t prepare_gemm() {
   cudaError_t e;
+  e = smem_attrs((const void *)tc::k_gemm_persist<MODE, A_MN, B_MN>, tc::kSmemP);
+  if (e != cudaSuccess) return e;
   e = smem_attrs((const void *)tc::k_gemm_split<MODE, A_MN, B_MN, 1>, tc::smem_bytes(1));
   if (e != cudaSuccess) return e;
   e = smem_attrs((const void *)tc::k_gemm_split<MODE, A_MN, B_MN, 2>, tc::smem_bytes(2));
@@ -1046,14 +1074,14 @@ int dg_handle::mixed_autotune() {
   // the warp form is the only one for odd or narrow grids; a user's choice stands
   const bool hydro_fixed = (hk && *hk) || X.hydro_kind == MixedState::kHydroWarp;
   // DISKGPU_STAGES=s0,s1,s2,s3,s4,s5 fixes the pipeline depth of every gravity product
-  // (0 = chosen by K, else 1, 2 or 4) and skips their tuning
+  // (0 = chosen by K, else 1, 2 or 4; 8 = the persistent kernel) and skips their tuning
   bool stages_fixed = false;
   if (const char *sv = getenv("DISKGPU_STAGES")) {
     int v[6], n = sscanf(sv, "%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]);
     if (n != 6) return fail(DG_ERR_INVALID, "autotune", "DISKGPU_STAGES wants six comma-separated depths");
     for (int k = 0; k < 6; ++k) {
-      if (v[k] != 0 && v[k] != 1 && v[k] != 2 && v[k] != 4)
-        return fail(DG_ERR_INVALID, "autotune", "DISKGPU_STAGES: a depth is 0, 1, 2 or 4");
+      if (v[k] != 0 && v[k] != 1 && v[k] != 2 && v[k] != 4 && v[k] != kPersist)
+        return fail(DG_ERR_INVALID, "autotune", "DISKGPU_STAGES: a depth is 0, 1, 2, 4 or 8 (persistent)");
       X.ns[k] = v[k];
     }
     stages_fixed = true;
@@ -1066,6 +1094,11 @@ int dg_handle::mixed_autotune() {
       if (!hydro_fixed) X.hydro_kind = it->second.hydro_kind;
       if (!stages_fixed) memcpy(X.ns, it->second.ns, sizeof(X.ns));
       X.tune_info = it->second.info + " (cached)";
+      if (stages_fixed && p.selfgrav) {  // the fixed depths, not the cached ones, are in use
+        std::string f = "gravity stages fixed";
+        for (int k = 0; k < 6; ++k) f += " " + std::to_string(X.ns[k]);
+        X.tune_info = f + "; " + X.tune_info;
+      }
       return DG_OK;
     }
   }
@@ -1113,7 +1146,7 @@ int dg_handle::mixed_autotune() {
       const float t0 = tbest;
       for (int sl : slots) {
         int keep = X.ns[sl];
-        for (int cand : {1, 2, 4}) {
+        for (int cand : {1, 2, 4, kPersist}) {
           X.ns[sl] = cand;
           float t;
           if ((e = time_us(grav, &t)) != cudaSuccess) break;
@@ -1289,10 +1322,10 @@ int dg_handle::mixed_gravity() {
       // S1: real 64-point DFT over j1 (s read as [(i, j1)][j2]), x W_N^{j2 m1} -> T[(m1, i)][(ri, j2)]
       a.out_hi = X.PhT.hi; a.out_lo = X.PhT.lo; a.twiddle = X.twph;
       XK((gemm<tc::kEpiPhiS1, false, true>(X.mPhA1[0], X.mPhA1[1], X.mSxBlk[0], X.mSxBlk[1], 128, Nu * 64, 64, a,
-                                             st, 0)));
+                                             st, X.ns[0])));
       // S2: complex 64-point DFT over j2 -> modes m = m1 + 64 m2 <= N/2 into Xin
       a.out_hi = X.Xin.hi; a.out_lo = X.Xin.lo;
-      XK(gemm<tc::kEpiPhiS2>(X.mPhT[0], X.mPhT[1], X.mPhB2f[0], X.mPhB2f[1], 64 * Nu, 128, 128, a, st, 0));
+      XK(gemm<tc::kEpiPhiS2>(X.mPhT[0], X.mPhT[1], X.mPhB2f[0], X.mPhB2f[1], 64 * Nu, 128, 128, a, st, X.ns[0]));
       a.twiddle = X.tw;
     } else {
       XK(gemm<tc::kEpiPhiToXin>(X.mFphi[0], X.mFphi[1], X.mSx[0], X.mSx[1], Nphi, Nu, Nphi, a, st, X.ns[0]));
@@ -1340,11 +1373,11 @@ int dg_handle::mixed_gravity() {
       // Q1: inverse 64-point DFT over m2 (X read MN-major), x W_N^{-j2 m1} -> V[(i, m1)][(ri, j2)]
       a.out_hi = X.PhV.hi; a.out_lo = X.PhV.lo; a.twiddle = X.twph;
       XK((gemm<tc::kEpiPhiQ1, true, false>(X.mPhX[0], X.mPhX[1], X.mPhB1i[0], X.mPhB1i[1], 64 * Nu, 128, 128, a,
-                                            st, 0)));
+                                            st, X.ns[5])));
       // Q2: real part of the inverse 64-point DFT over m1, / N, x (-G du dphi / sqrt(R))
       a.out_hi = a.out_lo = nullptr; a.out_f32 = X.dPhi; a.row_scale = X.phiscale;
       XK((gemm<tc::kEpiPhiQ2, true, false>(X.mPhV[0], X.mPhV[1], X.mPhB2i[0], X.mPhB2i[1], 64 * Nu, 64, 128, a,
-                                            st, 0)));
+                                            st, X.ns[5])));
     } else if (X.fused_phi) {
       tc::PhiInvArgs f{X.Zt.hi, X.Zt.lo, X.twphi, X.phiscale, X.dPhi, Nphi, &ctl->status, rp, rp_n, rp_val};
       XK(launch_pdl(tc::k_phiinv, dim3(Nu / tc::kPiRows), dim3(tc::kPiThreads), tc::kPiSmem, st, X.mIA[0], X.mIA[1],
@@ -1538,13 +1571,13 @@ struct MixedGroup {
   tc::PhiInvArgs *pi = nullptr;
 };
 
-std::string mixed_group_key(const dg_handle *h) {
+std::string mixed_group_key(const dg_handle *h, bool with_fused) {
   if (!h || h->p.precision != DG_PREC_MIXED || !h->p.selfgrav || !h->mx || !h->mx->tables_ready ||
       !h->have_state)
     return std::string();
   const MixedState &X = *h->mx;
   // dense products, or the fused 1024^2 transforms (the other factored forms step alone)
-  if (X.factored && !X.fused_phi) return std::string();
+  if (X.factored && (!X.fused_phi || !with_fused)) return std::string();
   if (X.hydro_kind != MixedState::kHydroPacked && X.hydro_kind != MixedState::kHydroTile) return std::string();
   char b[160];
   snprintf(b, sizeof b, "%d:%d:%d:%d:%d:%d:%d,%d,%d,%d", h->dev, X.Nu, X.Nphi, X.fused_phi ? 1 : 0, X.rows.gamma2,

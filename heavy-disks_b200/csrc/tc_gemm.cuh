@@ -721,9 +721,9 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 }
 
 template <int MODE, bool A_MN, bool B_MN, bool PER_A>
-__global__ void __launch_bounds__(kThreadsP, 1)
-    k_gemm_group_persist(const __grid_constant__ CUtensorMap tmCh, const __grid_constant__ CUtensorMap tmCl,
-                         const GemmDisk *__restrict__ disks, int tiles_n, int tiles_m, int ntiles) {
+__device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const CUtensorMap *pCl,
+                                                  const GemmDisk *__restrict__ disks, int tiles_n, int tiles_m,
+                                                  int ntiles) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ __align__(8) uint64_t full_bar[NS2], empty_bar[NS2], acc_full[2], acc_empty[2];
@@ -749,6 +749,8 @@ __global__ void __launch_bounds__(kThreadsP, 1)
   const uint32_t tmem = tmem_slot;
   pdl_wait();  // operands come from the previous kernel on the stream
   pdl_trigger();
+  if (disks[0].args.rowpend && blockIdx.x == 0)  // a lone product that arms the hydro's row tiles
+    for (int r = threadIdx.x; r < disks[0].args.rp_n; r += blockDim.x) disks[0].args.rowpend[r] = disks[0].args.rp_val;
   const int per_disk = tiles_n * tiles_m;
   auto decode = [&](int t, int &z, int &m0, int &n0) {
     z = t / per_disk;
@@ -767,8 +769,8 @@ __global__ void __launch_bounds__(kThreadsP, 1)
         decode(t, z, m0, n0);
         const GemmDisk &d = disks[z];
         st_word = d.args.status;
-        const CUtensorMap *Ah = PER_A ? &d.hi : &tmCh, *Al = PER_A ? &d.lo : &tmCl;
-        const CUtensorMap *Bh = PER_A ? &tmCh : &d.hi, *Bl = PER_A ? &tmCl : &d.lo;
+        const CUtensorMap *Ah = PER_A ? &d.hi : pCh, *Al = PER_A ? &d.lo : pCl;
+        const CUtensorMap *Bh = PER_A ? pCh : &d.hi, *Bl = PER_A ? pCl : &d.lo;
         const int nk = d.args.K / BK;
         for (int kc = 0; kc < nk; ++kc) {
           const uint32_t sidx = it % NS2;
@@ -779,7 +781,12 @@ __global__ void __launch_bounds__(kThreadsP, 1)
           if (abort_flag) break;
           uint8_t *st = smem + sidx * kStageBytes2;
           mbar_arrive_expect_tx(&full_bar[sidx], kStageBytes2);
-          if (A_MN) {
+          if (A_MN && MODE == kEpiPhiQ2) {  // V as [(i, m1, ri)][j2]: M chunk c = row i = m0 / 64 + c
+            tma_load_2d(st, Ah, &full_bar[sidx], 0, (m0 / 64) * 128 + kc * BK);
+            tma_load_2d(st + kTileA / 2, Ah, &full_bar[sidx], 0, (m0 / 64 + 1) * 128 + kc * BK);
+            tma_load_2d(st + kTileA, Al, &full_bar[sidx], 0, (m0 / 64) * 128 + kc * BK);
+            tma_load_2d(st + kTileA + kTileA / 2, Al, &full_bar[sidx], 0, (m0 / 64 + 1) * 128 + kc * BK);
+          } else if (A_MN) {
             tma_load_2d(st, Ah, &full_bar[sidx], m0, kc * BK);
             tma_load_2d(st + kTileA / 2, Ah, &full_bar[sidx], m0 + 64, kc * BK);
             tma_load_2d(st + kTileA, Al, &full_bar[sidx], m0, kc * BK);
@@ -791,7 +798,10 @@ __global__ void __launch_bounds__(kThreadsP, 1)
           uint8_t *sb = st + 2 * kTileA;
 #pragma unroll
           for (int c = 0; c < 2; ++c) {  // two 64-wide N chunks (MN-major) or 64-row boxes (K-major)
-            if (B_MN) {
+            if (B_MN && MODE == kEpiPhiS1) {  // the [(i, j1)][j2] view of s: N chunk = row i's 64 columns
+              tma_load_2d(sb + c * (kTileB2 / 2), Bh, &full_bar[sidx], 0, n0 + 64 * c + kc * BK);
+              tma_load_2d(sb + kTileB2 + c * (kTileB2 / 2), Bl, &full_bar[sidx], 0, n0 + 64 * c + kc * BK);
+            } else if (B_MN) {
               tma_load_2d(sb + c * (kTileB2 / 2), Bh, &full_bar[sidx], n0 + 64 * c, kc * BK);
               tma_load_2d(sb + kTileB2 + c * (kTileB2 / 2), Bl, &full_bar[sidx], n0 + 64 * c, kc * BK);
             } else {
@@ -881,6 +891,23 @@ __global__ void __launch_bounds__(kThreadsP, 1)
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, kTmemColsP);
+}
+
+template <int MODE, bool A_MN, bool B_MN, bool PER_A>
+__global__ void __launch_bounds__(kThreadsP, 1)
+    k_gemm_group_persist(const __grid_constant__ CUtensorMap tmCh, const __grid_constant__ CUtensorMap tmCl,
+                         const GemmDisk *__restrict__ disks, int tiles_n, int tiles_m, int ntiles) {
+  gemm_persist_body<MODE, A_MN, B_MN, PER_A>(&tmCh, &tmCl, disks, tiles_n, tiles_m, ntiles);
+}
+
+// One product of a lone disk by the persistent kernel: A's maps as kernel parameters, B's
+// maps and the epilogue arguments as one by-value entry (a "group" of one disk whose
+// tensor maps TMA reads from the parameter space).
+template <int MODE, bool A_MN, bool B_MN>
+__global__ void __launch_bounds__(kThreadsP, 1)
+    k_gemm_persist(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
+                   const __grid_constant__ GemmDisk b, int tiles_n, int tiles_m, int ntiles) {
+  gemm_persist_body<MODE, A_MN, B_MN, false>(&tmAh, &tmAl, &b, tiles_n, tiles_m, ntiles);
 }
 
 }  // namespace tc

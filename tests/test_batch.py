@@ -74,7 +74,8 @@ def test_grouped_1024_disks_equal_lone(monkeypatch):
     """Five 1024^2 sweep disks (two pairs that share a physics point and differ in seed
     phase and amplitude, so each pair is one step-rate class): grouped, the fused phi
     transform, u convolution and inverse phi transform run once per step for the whole
-    group (blockIdx.y = disk).  States bit for bit those with grouping off and those of a
+    group (blockIdx.y = disk; DISKGPU_BATCH_GROUPS=all, since 1024^2 disks step as branches
+    of their own by default).  States bit for bit those with grouping off and those of a
     lone run; step counts and times equal; mode records to 1e-12."""
     pts = S.draw(5, seed=3, grids=(1024,))
     params = [_params(p, "mixed") for p in pts]
@@ -83,13 +84,13 @@ def test_grouped_1024_disks_equal_lone(monkeypatch):
         params[k].phase0, params[k].amp = phase, amp
     tlim = 0.01
     out = {}
-    for grouped in ("1", "0"):
+    for grouped in ("all", "0"):
         monkeypatch.setenv("DISKGPU_BATCH_GROUPS", grouped)
         with D.Batch(params) as b:
             b.init_standard()
             recs, t, steps = b.advance(tlim, steps_per_launch=8, dtout=0.004)
             out[grouped] = ([d.get_state() for d in b.disks], recs, t, steps)
-    (sa, ra, ta, na), (sb, rb, tb, nb) = out["1"], out["0"]
+    (sa, ra, ta, na), (sb, rb, tb, nb) = out["all"], out["0"]
     assert np.array_equal(na, nb) and np.array_equal(ta, tb)
     assert min(na) > 40
     for k in range(len(params)):
