@@ -13,7 +13,9 @@
 // separate branches overlap one disk's transforms with another's hydro and keep each
 // disk's row-tile hand-over, which measured faster than the grouped kernels (2.05e10
 // against 1.93e10 zone-updates/s for 16 disks).  DISKGPU_BATCH_GROUPS=0 turns grouping
-// off (every disk its own branch).
+// off (every disk its own branch).  DISKGPU_BATCH_GRAPH=0 enqueues each launch's kernels
+// directly on the branches' streams instead of replaying the captured graph (the same
+// kernels, fork and join; for profilers that see only kernels launched outside graphs).
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -31,6 +33,9 @@ struct dg_batch {
   cudaGraphExec_t exec = nullptr;
   std::vector<cudaEvent_t> events;
   std::vector<MixedGroup *> groups;  // the groups the captured graph launches
+  std::vector<std::vector<int>> branches;  // disks of each branch (a group or one disk)
+  bool prepared = false;  // branches, groups and (unless direct) the graph are built
+  bool direct = false;    // DISKGPU_BATCH_GRAPH=0: launch the branches' kernels without a graph
   int dev = -1;
   std::string err;
   int fail(int code, const char *what, const char *why) {
@@ -42,6 +47,8 @@ struct dg_batch {
     exec = nullptr;
     for (MixedGroup *g : groups) mixed_group_destroy(g);
     groups.clear();
+    branches.clear();
+    prepared = false;
   }
 };
 
@@ -50,6 +57,35 @@ struct dg_batch {
     cudaError_t e_ = (call);                                                           \
     if (e_ != cudaSuccess) return b->fail(DG_ERR_CUDA, #call, cudaGetErrorString(e_)); \
   } while (0)
+
+// One launch's work: root -> fork to every branch's stream -> its steps -> join.  Recorded
+// once into the batch's graph, or (direct mode) enqueued as it is at every launch.
+static int batch_enqueue(dg_batch *b) {
+  const int n = (int)b->disks.size();
+  cudaError_t e = cudaEventRecord(b->events[n], b->root);
+  if (e != cudaSuccess) return b->fail(DG_ERR_CUDA, "dg_batch_advance", cudaGetErrorString(e));
+  size_t gi = 0;
+  for (size_t q = 0; q < b->branches.size(); ++q) {
+    const std::vector<int> &br = b->branches[q];
+    dg_handle *h = b->disks[br[0]];
+    int steps = 0;
+    for (int k : br) steps = std::max(steps, b->steps_per_launch[k]);
+    cudaStreamWaitEvent(h->st, b->events[n], 0);
+    int rc = DG_OK;
+    if (br.size() > 1) {
+      MixedGroup *grp = b->groups[gi++];
+      for (int s = 0; s < steps && !rc; ++s) rc = mixed_group_enqueue_step(grp, h->st);
+    } else {
+      for (int s = 0; s < steps && !rc; ++s) rc = h->enqueue_step();
+    }
+    if (rc) return b->fail(rc, "dg_batch_advance", h->err.c_str());
+    cudaEventRecord(b->events[q], h->st);
+    cudaStreamWaitEvent(b->root, b->events[q], 0);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return b->fail(DG_ERR_CUDA, "dg_batch_advance", cudaGetErrorString(e));
+  return DG_OK;
+}
 
 extern "C" {
 
@@ -146,7 +182,7 @@ int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int ste
     if (rc) return b->fail(rc, "dg_batch_advance", h->err.c_str());
   }
   // steps per launch: proportional to each disk's step rate (1/dt), even, at least 2
-  if (!b->exec) {
+  if (!b->prepared) {
     double dtmin = 1e300;
     for (dg_handle *h : b->disks) dtmin = std::min(dtmin, h->hctl->dt > 0 ? h->hctl->dt : 1e300);
     b->steps_per_launch.assign(n, steps_per_launch);
@@ -159,7 +195,8 @@ int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int ste
       b->steps_per_launch[k] = s;
     }
     // branches: groups of same-grid mixed disks, and lone disks
-    std::vector<std::vector<int>> branches;
+    std::vector<std::vector<int>> &branches = b->branches;
+    branches.clear();
     {
       const char *ge = getenv("DISKGPU_BATCH_GROUPS");
       const bool grouping = !(ge && strcmp(ge, "0") == 0);
@@ -191,44 +228,30 @@ int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int ste
         branches.emplace_back(std::move(kv.second));
       }
     }
-    // capture: root -> fork to every branch's stream -> its steps -> join
     for (dg_handle *h : b->disks) {
       int rc0 = h->prof_collect();
       if (rc0) return b->fail(rc0, "dg_batch_advance", h->err.c_str());
-      h->prof_on = false;  // no event timing inside the batch graph
+      h->prof_on = false;  // no event timing inside the batch's launches
     }
-    b->events.resize(n + 1);
-    cudaGraph_t g = nullptr;
-    BK(cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal));
-    cudaEventRecord(b->events[n], b->root);
-    int rc = DG_OK;
-    size_t gi = 0;
-    for (size_t q = 0; q < branches.size() && !rc; ++q) {
-      const std::vector<int> &br = branches[q];
-      dg_handle *h = b->disks[br[0]];
-      int steps = 0;
-      for (int k : br) steps = std::max(steps, b->steps_per_launch[k]);
-      cudaStreamWaitEvent(h->st, b->events[n], 0);
-      if (br.size() > 1) {
-        MixedGroup *grp = b->groups[gi++];
-        for (int s = 0; s < steps && !rc; ++s) rc = mixed_group_enqueue_step(grp, h->st);
-        if (rc) rc = b->fail(rc, "dg_batch_advance", h->err.c_str());
-      } else {
-        for (int s = 0; s < steps && !rc; ++s) rc = h->enqueue_step();
+    const char *gv = getenv("DISKGPU_BATCH_GRAPH");
+    b->direct = gv && strcmp(gv, "0") == 0;
+    if (!b->direct) {
+      // capture one launch's work as a graph
+      cudaGraph_t g = nullptr;
+      BK(cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal));
+      int rc = batch_enqueue(b);
+      cudaError_t e = cudaStreamEndCapture(b->root, &g);
+      for (dg_handle *h : b->disks) h->cur = 0;  // capture flipped the buffers an even number of times
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
       }
-      cudaEventRecord(b->events[q], h->st);
-      cudaStreamWaitEvent(b->root, b->events[q], 0);
+      BK(e);
+      e = cudaGraphInstantiate(&b->exec, g, 0);
+      cudaGraphDestroy(g);
+      BK(e);
     }
-    cudaError_t e = cudaStreamEndCapture(b->root, &g);
-    for (dg_handle *h : b->disks) h->cur = 0;  // capture flipped the buffers an even number of times
-    if (rc) {
-      if (g) cudaGraphDestroy(g);
-      return b->fail(rc, "dg_batch_advance", "capture");
-    }
-    BK(e);
-    e = cudaGraphInstantiate(&b->exec, g, 0);
-    cudaGraphDestroy(g);
-    BK(e);
+    b->prepared = true;
   }
   std::vector<double> tmp;
   for (;;) {
@@ -259,7 +282,12 @@ int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int ste
       if (h->t < tlim) running = true;
     }
     if (!running) break;
-    BK(cudaGraphLaunch(b->exec, b->root));
+    if (b->direct) {
+      int rc = batch_enqueue(b);  // every step count is even: each disk ends on buffer 0
+      if (rc) return rc;
+    } else {
+      BK(cudaGraphLaunch(b->exec, b->root));
+    }
   }
   for (int k = 0; k < n; ++k) {
     dg_handle *h = b->disks[k];

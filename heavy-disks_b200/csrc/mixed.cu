@@ -616,7 +616,8 @@ static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUte
       tc::GemmDisk b;
       b.hi = Bh; b.lo = Bl; b.args = a;
       const int tn = N / tc::BN2, tm = M / tc::BM, nt = tn * tm, nsm = sm_count();
-      return launch_pdl(tc::k_gemm_persist<MODE, A_MN, B_MN>, dim3(nt < nsm ? nt : nsm), dim3(tc::kThreadsP),
+      return launch_pdl(tc::k_gemm_persist<MODE, A_MN, B_MN>, dim3(nt < nsm ? nt : nsm),
+                        dim3(tc::threads_persist(tc::kEpiWarpsLone)),
                         tc::kSmemP, st, Ah, Al, b, tn, tm, nt);
     }
     ns = 0;  // N not a multiple of 128: the tile kernel, stages by K
@@ -1594,7 +1595,8 @@ static cudaError_t gemm_group(const CUtensorMap &Ch, const CUtensorMap &Cl, cons
     auto kp = tc::k_gemm_group_persist<MODE, A_MN, B_MN, PER_A>;
     if (prepare) return smem_attrs((const void *)kp, tc::kSmemP);
     const int tn = N / tc::BN2, tm = M / tc::BM, nt = tn * tm * G;
-    return launch_pdl(kp, dim3(nt < nsm ? nt : nsm), dim3(tc::kThreadsP), tc::kSmemP, st, Ch, Cl, d, tn, tm, nt);
+    return launch_pdl(kp, dim3(nt < nsm ? nt : nsm), dim3(tc::threads_persist(tc::kEpiWarpsGroup)), tc::kSmemP, st,
+                      Ch, Cl, d, tn, tm, nt);
   }
   const int nk = K / tc::BK;
   if (ns == 0) ns = nk <= 1 ? 1 : (nk <= 2 ? 2 : tc::STAGES);

@@ -701,9 +701,13 @@ __global__ void __launch_bounds__(kThreads, (NS == 1 ? 4 : (NS == 2 ? 2 : 1)))
 // Persistent form of the group product (batched sweeps).  One CTA per SM walks the tiles
 // of every disk of the group (tile t = blockIdx.x + k gridDim.x; disk, M tile, N tile
 // from t) with its warps specialised: warp 0 drives TMA through an NS2-deep ring of stages
-// that runs ahead across tile boundaries, warp 1 issues the MMAs, warps 2..5 drain TMEM
-// and run the epilogue.  Two TMEM accumulators (128 columns each) let the epilogue of one
-// tile overlap the MMAs of the next.  Tiles are 128 x 128: per byte loaded from L2 twice
+// that runs ahead across tile boundaries, warp 1 issues the MMAs, the other EW warps drain
+// TMEM and run the epilogue (EW / 4 warps per 32-lane TMEM quarter, each taking its share
+// of the tile's columns).  Two TMEM accumulators (128 columns each) let the epilogue of
+// one tile overlap the MMAs of the next.  A lone disk's products run with EW = 8: its
+// four-step and factored passes, one or two K blocks per tile with heavy epilogues, are
+// epilogue-bound.  The batch groups' dense products keep EW = 4, which measured about
+// 5 % faster for them.  Tiles are 128 x 128: per byte loaded from L2 twice
 // the MMA work of the 128 x 64 tiles above.  Each output element sees the same sequence
 // of K steps and products as in k_gemm_split.  All waits are bounded as above; on a
 // timeout every role stops at its next wait, in-flight copies are drained, and TMEM is
@@ -712,7 +716,8 @@ constexpr int BN2 = 128;
 constexpr int NS2 = 3;
 constexpr uint32_t kTileB2 = BN2 * BK * 2;
 constexpr uint32_t kStageBytes2 = 2 * kTileA + 2 * kTileB2;  // 64 KB
-constexpr int kThreadsP = 192;
+constexpr int kEpiWarpsLone = 8, kEpiWarpsGroup = 4;  // epilogue warps of the two entries
+constexpr int threads_persist(int ew) { return 64 + 32 * ew; }
 constexpr uint32_t kTmemColsP = 2 * BN2;
 constexpr size_t kSmemP = (size_t)NS2 * kStageBytes2 + 1024;
 
@@ -720,10 +725,11 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-template <int MODE, bool A_MN, bool B_MN, bool PER_A>
+template <int MODE, bool A_MN, bool B_MN, bool PER_A, int EW>
 __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const CUtensorMap *pCl,
                                                   const GemmDisk *__restrict__ disks, int tiles_n, int tiles_m,
                                                   int ntiles) {
+  static_assert(EW % 4 == 0 && BN2 % (32 * (EW / 4)) == 0, "epilogue warps cover the tile");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   __shared__ __align__(8) uint64_t full_bar[NS2], empty_bar[NS2], acc_full[2], acc_empty[2];
@@ -737,7 +743,7 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
     }
     for (int q = 0; q < 2; ++q) {
       mbar_init(&acc_full[q], 1);
-      mbar_init(&acc_empty[q], 4);  // one arrival per epilogue warp
+      mbar_init(&acc_empty[q], EW);  // one arrival per epilogue warp
     }
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -863,8 +869,10 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
       }
     }
   } else {
-    // ---- epilogue: warp w drains TMEM lanes 32 (w % 4) .. + 31 ----
+    // ---- epilogue: warp w drains TMEM lanes 32 (w % 4) .. + 31, columns of its half ----
     const int qd = warp & 3;
+    constexpr int kCols = BN2 / (EW / 4);
+    const int cb = ((warp - 2) / 4) * kCols;
     int lt = 0;
     for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++lt) {
       int z, m0, n0;
@@ -878,7 +886,7 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
       tc_fence_after();
       const int row = m0 + qd * 32 + lane;
 #pragma unroll 1
-      for (int c0 = 0; c0 < BN2; c0 += 32) {
+      for (int c0 = cb; c0 < cb + kCols; c0 += 32) {
         uint32_t r[32];
         tmem_ld32(tmem + (uint32_t)(buf * BN2) + ((uint32_t)(qd * 32) << 16) + (uint32_t)c0, r);
         epi_chunk<MODE>(d.args, row, n0 + c0, r, lane);
@@ -894,20 +902,20 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
 }
 
 template <int MODE, bool A_MN, bool B_MN, bool PER_A>
-__global__ void __launch_bounds__(kThreadsP, 1)
+__global__ void __launch_bounds__(threads_persist(kEpiWarpsGroup), 1)
     k_gemm_group_persist(const __grid_constant__ CUtensorMap tmCh, const __grid_constant__ CUtensorMap tmCl,
                          const GemmDisk *__restrict__ disks, int tiles_n, int tiles_m, int ntiles) {
-  gemm_persist_body<MODE, A_MN, B_MN, PER_A>(&tmCh, &tmCl, disks, tiles_n, tiles_m, ntiles);
+  gemm_persist_body<MODE, A_MN, B_MN, PER_A, kEpiWarpsGroup>(&tmCh, &tmCl, disks, tiles_n, tiles_m, ntiles);
 }
 
 // One product of a lone disk by the persistent kernel: A's maps as kernel parameters, B's
 // maps and the epilogue arguments as one by-value entry (a "group" of one disk whose
 // tensor maps TMA reads from the parameter space).
 template <int MODE, bool A_MN, bool B_MN>
-__global__ void __launch_bounds__(kThreadsP, 1)
+__global__ void __launch_bounds__(threads_persist(kEpiWarpsLone), 1)
     k_gemm_persist(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                    const __grid_constant__ GemmDisk b, int tiles_n, int tiles_m, int ntiles) {
-  gemm_persist_body<MODE, A_MN, B_MN, false>(&tmAh, &tmAl, &b, tiles_n, tiles_m, ntiles);
+  gemm_persist_body<MODE, A_MN, B_MN, false, kEpiWarpsLone>(&tmAh, &tmAl, &b, tiles_n, tiles_m, ntiles);
 }
 
 }  // namespace tc

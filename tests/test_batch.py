@@ -103,3 +103,24 @@ def test_grouped_1024_disks_equal_lone(monkeypatch):
         d.advance(tlim, dtout=0.004)
         for x, y in zip(sa[2], d.get_state()):
             assert np.array_equal(x, y)
+
+
+def test_direct_launches_equal_graph_replay(monkeypatch):
+    """DISKGPU_BATCH_GRAPH=0 enqueues every launch's kernels directly (for profilers that
+    see only kernels launched outside graphs): the same kernels in the same order, so the
+    states equal the graph-replayed batch's bit for bit, with the same step counts."""
+    pts = S.draw(6, seed=5, grids=(128, 256))
+    params = [_params(p, "mixed") for p in pts]
+    out = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("DISKGPU_BATCH_GRAPH", mode)
+        with D.Batch(params) as b:
+            b.init_standard()
+            recs, t, steps = b.advance(0.05, steps_per_launch=8, dtout=0.02)
+            out[mode] = ([d.get_state() for d in b.disks], recs, t, steps)
+    (sa, ra, ta, na), (sb, rb, tb, nb) = out["1"], out["0"]
+    assert np.array_equal(na, nb) and np.array_equal(ta, tb)
+    for k in range(len(params)):
+        for x, y in zip(sa[k], sb[k]):
+            assert np.array_equal(x, y), k
+        np.testing.assert_allclose(ra[k], rb[k], rtol=1e-12, atol=1e-15)
