@@ -228,6 +228,27 @@ int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int ste
         branches.emplace_back(std::move(kv.second));
       }
     }
+    {
+      // the branches with the most work (zones x steps per launch) are enqueued first
+      std::vector<std::pair<std::vector<int>, MixedGroup *>> order;
+      size_t gi = 0;
+      for (auto &br : branches) order.emplace_back(br, br.size() > 1 ? b->groups[gi++] : nullptr);
+      auto work = [&](const std::vector<int> &br) {
+        double w = 0;
+        int steps = 0;
+        for (int k : br) steps = std::max(steps, b->steps_per_launch[k]);
+        for (int k : br) w += (double)b->disks[k]->p.Nu * b->disks[k]->p.Nphi;
+        return w * steps;
+      };
+      std::stable_sort(order.begin(), order.end(),
+                       [&](const auto &x, const auto &y) { return work(x.first) > work(y.first); });
+      branches.clear();
+      b->groups.clear();
+      for (auto &o : order) {
+        branches.push_back(o.first);
+        if (o.second) b->groups.push_back(o.second);
+      }
+    }
     for (dg_handle *h : b->disks) {
       int rc0 = h->prof_collect();
       if (rc0) return b->fail(rc0, "dg_batch_advance", h->err.c_str());
