@@ -83,12 +83,14 @@ def parse():
                          "momentum drift (0: skip)")
     ap.add_argument("--batch-disks", type=int, default=256,
                     help="disks of the batched sweep measurement (0: skip it)")
-    ap.add_argument("--batch-tlim", type=float, default=0.1, help="time the batched sweep advances")
+    ap.add_argument("--batch-tlim", type=float, default=0.5,
+                    help="time the batched sweep advances (long enough that the last launch's pass-through "
+                         "steps of disks already at tlim are a small part of the timed region)")
     ap.add_argument("--batch-grids", default="128,256,384,512", help="grid sizes the batch draws from")
     ap.add_argument("--batch-seed", type=int, default=12345, help="seed of the batch's sweep-law draw")
     ap.add_argument("--batch1024-disks", type=int, default=16,
                     help="disks of the batched 1024^2 measurement (sweep-law physics, every grid 1024^2; 0: skip)")
-    ap.add_argument("--batch1024-tlim", type=float, default=0.05, help="time the batched 1024^2 disks advance")
+    ap.add_argument("--batch1024-tlim", type=float, default=0.25, help="time the batched 1024^2 disks advance")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 

@@ -16,6 +16,8 @@
 // off (every disk its own branch).  DISKGPU_BATCH_GRAPH=0 enqueues each launch's kernels
 // directly on the branches' streams instead of replaying the captured graph (the same
 // kernels, fork and join; for profilers that see only kernels launched outside graphs).
+// DISKGPU_BATCH_LANES=K keeps at most K branches of a launch in flight (branch q starts
+// when branch q - K ends), to bound a launch's working set.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -36,6 +38,7 @@ struct dg_batch {
   std::vector<std::vector<int>> branches;  // disks of each branch (a group or one disk)
   bool prepared = false;  // branches, groups and (unless direct) the graph are built
   bool direct = false;    // DISKGPU_BATCH_GRAPH=0: launch the branches' kernels without a graph
+  int lanes = 0;          // branches in flight at once (0: all); DISKGPU_BATCH_LANES
   int dev = -1;
   std::string err;
   int fail(int code, const char *what, const char *why) {
@@ -70,7 +73,10 @@ static int batch_enqueue(dg_batch *b) {
     dg_handle *h = b->disks[br[0]];
     int steps = 0;
     for (int k : br) steps = std::max(steps, b->steps_per_launch[k]);
-    cudaStreamWaitEvent(h->st, b->events[n], 0);
+    // with lanes, branch q follows branch q - lanes (its lane's previous one) instead of
+    // starting at the fork, so at most `lanes` branches are in flight at once
+    const size_t lanes = b->lanes > 0 ? (size_t)b->lanes : b->branches.size();
+    cudaStreamWaitEvent(h->st, q < lanes ? b->events[n] : b->events[q - lanes], 0);
     int rc = DG_OK;
     if (br.size() > 1) {
       MixedGroup *grp = b->groups[gi++];
@@ -256,6 +262,8 @@ int dg_batch_advance(dg_batch *b, double tlim, double cfl, double dtout, int ste
     }
     const char *gv = getenv("DISKGPU_BATCH_GRAPH");
     b->direct = gv && strcmp(gv, "0") == 0;
+    const char *lv = getenv("DISKGPU_BATCH_LANES");
+    b->lanes = lv ? std::max(0, atoi(lv)) : 0;
     if (!b->direct) {
       // capture one launch's work as a graph
       cudaGraph_t g = nullptr;

@@ -124,3 +124,24 @@ def test_direct_launches_equal_graph_replay(monkeypatch):
         for x, y in zip(sa[k], sb[k]):
             assert np.array_equal(x, y), k
         np.testing.assert_allclose(ra[k], rb[k], rtol=1e-12, atol=1e-15)
+
+
+def test_lanes_equal_unlimited_concurrency(monkeypatch):
+    """DISKGPU_BATCH_LANES=2 lets at most two branches of a launch run at once (each branch
+    follows the one two places before it): the same kernels per disk in the same order, so
+    the states equal the unlimited batch's bit for bit."""
+    pts = S.draw(7, seed=6, grids=(128, 256))
+    params = [_params(p, "mixed") for p in pts]
+    out = {}
+    for lanes in ("0", "2"):
+        monkeypatch.setenv("DISKGPU_BATCH_LANES", lanes)
+        with D.Batch(params) as b:
+            b.init_standard()
+            recs, t, steps = b.advance(0.05, steps_per_launch=8, dtout=0.02)
+            out[lanes] = ([d.get_state() for d in b.disks], recs, t, steps)
+    (sa, ra, ta, na), (sb, rb, tb, nb) = out["0"], out["2"]
+    assert np.array_equal(na, nb) and np.array_equal(ta, tb)
+    for k in range(len(params)):
+        for x, y in zip(sa[k], sb[k]):
+            assert np.array_equal(x, y), k
+        np.testing.assert_allclose(ra[k], rb[k], rtol=1e-12, atol=1e-15)
