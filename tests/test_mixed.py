@@ -109,6 +109,34 @@ def test_mixed_vs_fp64_after_steps(N, steps):
     assert np.max(np.abs(vp - vpr)) <= 2e-3 * np.max(np.abs(vpr - vp0)) + 1e-9
 
 
+@pytest.mark.parametrize("Nu,Nphi,steps,vtol", [(256, 384, 80, 2e-3), (384, 256, 80, 2e-3), (128, 512, 100, 2e-3),
+                                                (512, 128, 80, 2e-3), (1024, 2048, 30, 2e-3), (2048, 1024, 16, 1e-2)])
+def test_mixed_nonsquare_vs_fp64_after_steps(Nu, Nphi, steps, vtol):
+    """Non-square grids in lockstep with the FP64 oracle: the hydro tiles' partial last
+    column tile and periodic wrap at other widths than the radial extent, rectangular dense
+    products, the fused u convolution beside the dense phi products (1024 x 2048) and the
+    four-pass u convolution beside them (2048 x 1024).  Sigma within 2e-3 of the
+    perturbation's size everywhere; the velocities within 2e-3, except at 2048 x 1024,
+    where after 16 steps the velocity perturbation is still young and the split-BF16
+    potential's error (within the 2e-4 of the potential tests) is differenced over twice
+    the 1024^2 radial resolution: 1e-2 there (measured 4e-3)."""
+    ref = O.Disk(Nu=Nu, Nphi=Nphi, eps=0.005, amp=1e-3, nthreads=os.cpu_count() or 8)
+    S0 = ref.hyd.get("Sig").mean(axis=1, keepdims=True)
+    with D.Disk(Nu, Nphi, eps=0.005, amp=1e-3, precision="mixed") as d:
+        d.init_standard()
+        for _ in range(steps):
+            dt_ref = ref.step()
+            dt = d.timestep(0.3)
+            assert abs(dt - dt_ref) <= 1e-5 * dt_ref
+            d.step(dt_ref)
+        S, vR, vp = d.get_state()
+    Sr, vRr, vpr = ref.hyd.state()
+    assert np.max(np.abs(S - Sr)) <= 2e-3 * np.max(np.abs(Sr - S0))
+    assert np.max(np.abs(vR - vRr)) <= vtol * np.max(np.abs(vRr))
+    vp0 = vpr.mean(axis=1, keepdims=True)
+    assert np.max(np.abs(vp - vpr)) <= vtol * np.max(np.abs(vpr - vp0)) + 1e-9
+
+
 def test_growth_rate_and_pattern_speed_match_fp64():
     """gamma, Omega_p of the m=2 mode from mixed and FP64 runs of the same disk (<= 0.5 %)."""
     kw = dict(eps=0.01, amp=1e-3)
