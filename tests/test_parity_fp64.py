@@ -88,6 +88,26 @@ def test_fp64_vs_oracle_after_steps(N, steps):
     assert np.max(np.abs(vR - vRr)) < TOL * np.max(np.abs(vpr))
 
 
+@pytest.mark.parametrize("Nu,Nphi,steps", [(128, 384, 100), (384, 128, 60), (240, 180, 100)])
+def test_fp64_nonsquare_vs_oracle_after_steps(Nu, Nphi, steps):
+    """Non-square grids on the FP64 path, one of them with radix-3 and radix-5 transform
+    lengths (240 x 180: padded u length 480, phi length 180): <= 1e-10 relative after the
+    given steps, dt to 1e-11 every step."""
+    ref = O.Disk(nthreads=8, Nu=Nu, Nphi=Nphi, eps=0.005, amp=1e-3)
+    with D.Disk(Nu, Nphi, eps=0.005, amp=1e-3) as d:
+        d.init_standard()
+        for _ in range(steps):
+            dt_ref = ref.step()
+            dt = d.timestep(0.3)
+            assert abs(dt - dt_ref) <= 1e-11 * dt_ref
+            d.step(dt)
+        S, vR, vp = d.get_state()
+    Sr, vRr, vpr = ref.hyd.state()
+    assert rel_err(S, Sr) < TOL
+    assert rel_err(vp, vpr) < TOL
+    assert np.max(np.abs(vR - vRr)) < TOL * np.max(np.abs(vpr))
+
+
 def test_step_with_caller_forces_and_without_gravity():
     """DiskHydro::step(dt, gR, gp) with explicit forces, and with none."""
     rng = np.random.default_rng(3)
