@@ -47,6 +47,8 @@ def test_defaults_are_the_reference_cli_defaults():
 @pytest.mark.parametrize("kw,code", [
     (dict(Nu=1), -1), (dict(Nphi=1), -1), (dict(Rin=0.0), -1), (dict(Rout=0.1), -1),
     (dict(Nphi=14), -4), (dict(Nu=7), -4), (dict(precision=7), -1), (dict(eps=-1.0), -1),
+    (dict(Nu=8192), -4), (dict(Nphi=16384), -4),  # the largest grid is 4096 x 8192
+    (dict(gamma_gas=0.0), -1), (dict(Kpoly=-0.25), -1), (dict(Nphi=14 * 7), -4),
 ])
 def test_invalid_params_rejected_before_device(kw, code):
     with pytest.raises(D.DiskGPUError) as e:
