@@ -36,7 +36,7 @@ def test_batch_equals_individual_runs(precision):
         for a, c in zip(states[k], st1):
             assert np.array_equal(a, c)
         assert recs[k].shape == rec1.shape
-        assert np.allclose(recs[k], rec1, rtol=1e-12, atol=1e-15)
+        assert np.allclose(recs[k], rec1, rtol=1e-10, atol=1e-13)
 
 
 def test_grouped_batch_equals_ungrouped_and_lone(monkeypatch):
@@ -44,7 +44,8 @@ def test_grouped_batch_equals_ungrouped_and_lone(monkeypatch):
     form same-grid groups advanced by one launch per kernel (blockIdx.z = disk); the states
     are bit for bit the ones with grouping off (DISKGPU_BATCH_GROUPS=0, one graph branch
     per disk) and the ones of lone runs, the step counts and times equal; the mode records
-    agree to 1e-12 (their FP64 sums are folded with atomics in a varying order)."""
+    agree to 1e-10 (their FP64 sums are folded with atomics in a varying order; differences
+    of ~2e-12 occur)."""
     pts = S.draw(16, seed=3, grids=(128, 256, 384, 512))
     params = [_params(p, "mixed") for p in pts] + [_params(p, "fp64") for p in pts[:2]]
     tlim = 0.03
@@ -60,7 +61,7 @@ def test_grouped_batch_equals_ungrouped_and_lone(monkeypatch):
     for k in range(len(params)):
         for x, y in zip(sa[k], sb[k]):
             assert np.array_equal(x, y), k
-        np.testing.assert_allclose(ra[k], rb[k], rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(ra[k], rb[k], rtol=1e-10, atol=1e-13)
     for k in (0, 5, 16):
         p = params[k]
         with D.Disk(p.Nu, p.Nphi, params=p, precision="mixed" if p.precision == D.MIXED else "fp64") as d:
@@ -76,7 +77,7 @@ def test_grouped_1024_disks_equal_lone(monkeypatch):
     transform, u convolution and inverse phi transform run once per step for the whole
     group (blockIdx.y = disk; DISKGPU_BATCH_GROUPS=all, since 1024^2 disks step as branches
     of their own by default).  States bit for bit those with grouping off and those of a
-    lone run; step counts and times equal; mode records to 1e-12."""
+    lone run; step counts and times equal; mode records to 1e-10."""
     pts = S.draw(5, seed=3, grids=(1024,))
     params = [_params(p, "mixed") for p in pts]
     for k, src, phase, amp in ((2, 0, 2.3, 3e-3), (3, 1, 0.2, 2e-3)):
@@ -96,7 +97,7 @@ def test_grouped_1024_disks_equal_lone(monkeypatch):
     for k in range(len(params)):
         for x, y in zip(sa[k], sb[k]):
             assert np.array_equal(x, y), k
-        np.testing.assert_allclose(ra[k], rb[k], rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(ra[k], rb[k], rtol=1e-10, atol=1e-13)
     p = params[2]
     with D.Disk(p.Nu, p.Nphi, params=p, precision="mixed") as d:
         d.init_standard()
@@ -123,7 +124,7 @@ def test_direct_launches_equal_graph_replay(monkeypatch):
     for k in range(len(params)):
         for x, y in zip(sa[k], sb[k]):
             assert np.array_equal(x, y), k
-        np.testing.assert_allclose(ra[k], rb[k], rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(ra[k], rb[k], rtol=1e-10, atol=1e-13)
 
 
 def test_lanes_equal_unlimited_concurrency(monkeypatch):
@@ -144,4 +145,4 @@ def test_lanes_equal_unlimited_concurrency(monkeypatch):
     for k in range(len(params)):
         for x, y in zip(sa[k], sb[k]):
             assert np.array_equal(x, y), k
-        np.testing.assert_allclose(ra[k], rb[k], rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(ra[k], rb[k], rtol=1e-10, atol=1e-13)
