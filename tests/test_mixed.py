@@ -137,6 +137,34 @@ def test_mixed_nonsquare_vs_fp64_after_steps(Nu, Nphi, steps, vtol):
     assert np.max(np.abs(vp - vpr)) <= vtol * np.max(np.abs(vpr - vp0)) + 1e-9
 
 
+@pytest.mark.parametrize("Nu,Nphi", [(128, 128), (256, 384)])
+def test_mixed_caller_forces_and_no_gravity_vs_oracle(Nu, Nphi):
+    """The mixed hydro's other two force forms against the oracle stepped in lockstep:
+    30 steps with the caller's forces (DiskHydro::step(dt, gR, gp) through dg_step_forces:
+    the oracle's own Kalnajs forces of its current state, passed as FP64 arrays), then 30
+    with no force at all (DiskHydro::step(dt)).  The perturbation fields within 2e-3 of
+    their size."""
+    ref = O.Disk(Nu=Nu, Nphi=Nphi, eps=0.01, amp=1e-2, nthreads=os.cpu_count() or 8)
+    S0 = ref.hyd.get("Sig").mean(axis=1, keepdims=True)
+    with D.Disk(Nu, Nphi, eps=0.01, amp=1e-2, precision="mixed") as d:
+        d.init_standard()
+        for _ in range(30):
+            dt = ref.hyd.timestep(0.3)
+            gR, gp = ref.gravity()
+            ref.hyd.step(dt, gR, gp)
+            d.step_forces(dt, gR, gp)
+        for _ in range(30):
+            dt = ref.hyd.timestep(0.3)
+            ref.hyd.step(dt)
+            d.step_forces(dt)
+        S, vR, vp = d.get_state()
+    Sr, vRr, vpr = ref.hyd.state()
+    assert np.max(np.abs(S - Sr)) <= 2e-3 * np.max(np.abs(Sr - S0)), np.max(np.abs(S - Sr)) / np.max(np.abs(Sr - S0))
+    assert np.max(np.abs(vR - vRr)) <= 2e-3 * np.max(np.abs(vRr)), np.max(np.abs(vR - vRr)) / np.max(np.abs(vRr))
+    vp0 = vpr.mean(axis=1, keepdims=True)
+    assert np.max(np.abs(vp - vpr)) <= 2e-3 * np.max(np.abs(vpr - vp0)) + 1e-9
+
+
 def test_growth_rate_and_pattern_speed_match_fp64():
     """gamma, Omega_p of the m=2 mode from mixed and FP64 runs of the same disk (<= 0.5 %)."""
     kw = dict(eps=0.01, amp=1e-3)
