@@ -1591,6 +1591,19 @@ static cudaError_t gemm_group(const CUtensorMap &Ch, const CUtensorMap &Cl, cons
                               int N, int K, cudaStream_t st, int ns, bool prepare, bool persist = false,
                               int nsm = 148) {
   if (M % tc::BM || N % tc::BN || K % tc::BK) return cudaErrorInvalidValue;
+  // 128 x 256 tiles where N allows (half the bytes of the shared operand per flop; two
+  // pipeline stages), unless DISKGPU_GROUP_TILE=128
+  static const bool wide_ok = [] {
+    const char *v = getenv("DISKGPU_GROUP_TILE");
+    return !(v && strcmp(v, "128") == 0);
+  }();
+  if (persist && N % 256 == 0 && wide_ok) {
+    auto kp = tc::k_gemm_group_persist<MODE, A_MN, B_MN, PER_A, 256>;
+    if (prepare) return smem_attrs((const void *)kp, tc::smem_persist(256));
+    const int tn = N / 256, tm = M / tc::BM, nt = tn * tm * G;
+    return launch_pdl(kp, dim3(nt < nsm ? nt : nsm), dim3(tc::threads_persist(tc::kEpiWarpsGroup)),
+                      tc::smem_persist(256), st, Ch, Cl, d, tn, tm, nt);
+  }
   if (persist && N % tc::BN2 == 0) {
     auto kp = tc::k_gemm_group_persist<MODE, A_MN, B_MN, PER_A>;
     if (prepare) return smem_attrs((const void *)kp, tc::kSmemP);

@@ -720,24 +720,33 @@ constexpr int kEpiWarpsLone = 8, kEpiWarpsGroup = 4;  // epilogue warps of the t
 constexpr int threads_persist(int ew) { return 64 + 32 * ew; }
 constexpr uint32_t kTmemColsP = 2 * BN2;
 constexpr size_t kSmemP = (size_t)NS2 * kStageBytes2 + 1024;
+// pipeline stages and dynamic shared memory of the persistent kernel for a tile width
+__host__ __device__ constexpr int persist_stages(int bnt) { return bnt == 256 ? 2 : NS2; }
+__host__ __device__ constexpr size_t smem_persist(int bnt) {
+  return (size_t)persist_stages(bnt) * (2 * kTileA + 2 * (size_t)bnt * BK * 2) + 1024;
+}
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-template <int MODE, bool A_MN, bool B_MN, bool PER_A, int EW>
+template <int MODE, bool A_MN, bool B_MN, bool PER_A, int EW, int BNT>
 __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const CUtensorMap *pCl,
                                                   const GemmDisk *__restrict__ disks, int tiles_n, int tiles_m,
                                                   int ntiles) {
-  static_assert(EW % 4 == 0 && BN2 % (32 * (EW / 4)) == 0, "epilogue warps cover the tile");
+  // tile width BNT (128, or 256 with two stages and the whole TMEM for two accumulators)
+  constexpr int NST = persist_stages(BNT);
+  constexpr uint32_t kTB = (uint32_t)BNT * BK * 2, kSB = 2 * kTileA + 2 * kTB, kTC = 2 * BNT;
+  constexpr uint32_t kChunkB = 64 * BK * 2;  // one 64-wide N chunk (or 64-row box) of a B plane
+  static_assert(EW % 4 == 0 && BNT % (32 * (EW / 4)) == 0, "epilogue warps cover the tile");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) uint64_t full_bar[NS2], empty_bar[NS2], acc_full[2], acc_empty[2];
+  __shared__ __align__(8) uint64_t full_bar[NST], empty_bar[NST], acc_full[2], acc_empty[2];
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int q = 0; q < NS2; ++q) {
+    for (int q = 0; q < NST; ++q) {
       mbar_init(&full_bar[q], 1);
       mbar_init(&empty_bar[q], 1);
     }
@@ -748,7 +757,7 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) tmem_alloc(&tmem_slot, kTmemColsP);
+  if (warp == 0) tmem_alloc(&tmem_slot, kTC);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -762,7 +771,7 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
     z = t / per_disk;
     const int r = t - z * per_disk;
     m0 = (r / tiles_n) * BM;
-    n0 = (r - (r / tiles_n) * tiles_n) * BN2;
+    n0 = (r - (r / tiles_n) * tiles_n) * BNT;
   };
 
   if (warp == 0) {
@@ -779,14 +788,14 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
         const CUtensorMap *Bh = PER_A ? pCh : &d.hi, *Bl = PER_A ? pCl : &d.lo;
         const int nk = d.args.K / BK;
         for (int kc = 0; kc < nk; ++kc) {
-          const uint32_t sidx = it % NS2;
-          if (it >= NS2 && !mbar_wait(&empty_bar[sidx], ((it / NS2) - 1) & 1, st_word)) {
+          const uint32_t sidx = it % NST;
+          if (it >= NST && !mbar_wait(&empty_bar[sidx], ((it / NST) - 1) & 1, st_word)) {
             abort_flag = 1;
             break;
           }
           if (abort_flag) break;
-          uint8_t *st = smem + sidx * kStageBytes2;
-          mbar_arrive_expect_tx(&full_bar[sidx], kStageBytes2);
+          uint8_t *st = smem + sidx * kSB;
+          mbar_arrive_expect_tx(&full_bar[sidx], kSB);
           if (A_MN && MODE == kEpiPhiQ2) {  // V as [(i, m1, ri)][j2]: M chunk c = row i = m0 / 64 + c
             tma_load_2d(st, Ah, &full_bar[sidx], 0, (m0 / 64) * 128 + kc * BK);
             tma_load_2d(st + kTileA / 2, Ah, &full_bar[sidx], 0, (m0 / 64 + 1) * 128 + kc * BK);
@@ -803,28 +812,28 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
           }
           uint8_t *sb = st + 2 * kTileA;
 #pragma unroll
-          for (int c = 0; c < 2; ++c) {  // two 64-wide N chunks (MN-major) or 64-row boxes (K-major)
+          for (int c = 0; c < BNT / 64; ++c) {  // 64-wide N chunks (MN-major) or 64-row boxes (K-major)
             if (B_MN && MODE == kEpiPhiS1) {  // the [(i, j1)][j2] view of s: N chunk = row i's 64 columns
-              tma_load_2d(sb + c * (kTileB2 / 2), Bh, &full_bar[sidx], 0, n0 + 64 * c + kc * BK);
-              tma_load_2d(sb + kTileB2 + c * (kTileB2 / 2), Bl, &full_bar[sidx], 0, n0 + 64 * c + kc * BK);
+              tma_load_2d(sb + c * (kChunkB), Bh, &full_bar[sidx], 0, n0 + 64 * c + kc * BK);
+              tma_load_2d(sb + kTB + c * (kChunkB), Bl, &full_bar[sidx], 0, n0 + 64 * c + kc * BK);
             } else if (B_MN) {
-              tma_load_2d(sb + c * (kTileB2 / 2), Bh, &full_bar[sidx], n0 + 64 * c, kc * BK);
-              tma_load_2d(sb + kTileB2 + c * (kTileB2 / 2), Bl, &full_bar[sidx], n0 + 64 * c, kc * BK);
+              tma_load_2d(sb + c * (kChunkB), Bh, &full_bar[sidx], n0 + 64 * c, kc * BK);
+              tma_load_2d(sb + kTB + c * (kChunkB), Bl, &full_bar[sidx], n0 + 64 * c, kc * BK);
             } else {
-              tma_load_2d(sb + c * (kTileB2 / 2), Bh, &full_bar[sidx], kc * BK, n0 + 64 * c);
-              tma_load_2d(sb + kTileB2 + c * (kTileB2 / 2), Bl, &full_bar[sidx], kc * BK, n0 + 64 * c);
+              tma_load_2d(sb + c * (kChunkB), Bh, &full_bar[sidx], kc * BK, n0 + 64 * c);
+              tma_load_2d(sb + kTB + c * (kChunkB), Bl, &full_bar[sidx], kc * BK, n0 + 64 * c);
             }
           }
           ++it;
         }
       }
       // every issued copy must land before the CTA may exit
-      for (uint32_t j = it > NS2 ? it - NS2 : 0; j < it; ++j) mbar_wait(&full_bar[j % NS2], (j / NS2) & 1, st_word);
+      for (uint32_t j = it > NST ? it - NST : 0; j < it; ++j) mbar_wait(&full_bar[j % NST], (j / NST) & 1, st_word);
     }
   } else if (warp == 1) {
     if (lane == 0) {
       // ---- MMA issuer ----
-      const uint32_t idesc = idesc_bf16(BM, BN2, A_MN, B_MN);
+      const uint32_t idesc = idesc_bf16(BM, BNT, A_MN, B_MN);
       uint32_t it = 0;
       int lt = 0;
       for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++lt) {
@@ -838,22 +847,22 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
           break;
         }
         tc_fence_after();
-        const uint32_t acc = tmem + (uint32_t)(buf * BN2);
+        const uint32_t acc = tmem + (uint32_t)(buf * BNT);
         bool ok = true;
         for (int kc = 0; kc < nk; ++kc, ++it) {
-          const uint32_t sidx = it % NS2;
-          if (!mbar_wait(&full_bar[sidx], (it / NS2) & 1, d.args.status)) {
+          const uint32_t sidx = it % NST;
+          if (!mbar_wait(&full_bar[sidx], (it / NST) & 1, d.args.status)) {
             abort_flag = 1;
             ok = false;
             break;
           }
           tc_fence_after();
-          uint8_t *st = smem + sidx * kStageBytes2;
+          uint8_t *st = smem + sidx * kSB;
           const uint64_t dAh = A_MN ? sdesc_mn_sw128(st, kTileA / 2) : sdesc_sw128(st);
           const uint64_t dAl = A_MN ? sdesc_mn_sw128(st + kTileA, kTileA / 2) : sdesc_sw128(st + kTileA);
-          const uint64_t dBh = B_MN ? sdesc_mn_sw128(st + 2 * kTileA, kTileB2 / 2) : sdesc_sw128(st + 2 * kTileA);
+          const uint64_t dBh = B_MN ? sdesc_mn_sw128(st + 2 * kTileA, kChunkB) : sdesc_sw128(st + 2 * kTileA);
           const uint64_t dBl =
-              B_MN ? sdesc_mn_sw128(st + 2 * kTileA + kTileB2, kTileB2 / 2) : sdesc_sw128(st + 2 * kTileA + kTileB2);
+              B_MN ? sdesc_mn_sw128(st + 2 * kTileA + kTB, kChunkB) : sdesc_sw128(st + 2 * kTileA + kTB);
           const uint64_t stepA = A_MN ? (2048 >> 4) : (32 >> 4), stepB = B_MN ? (2048 >> 4) : (32 >> 4);
 #pragma unroll
           for (int kk = 0; kk < BK / 16; ++kk) {
@@ -871,7 +880,7 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
   } else {
     // ---- epilogue: warp w drains TMEM lanes 32 (w % 4) .. + 31, columns of its half ----
     const int qd = warp & 3;
-    constexpr int kCols = BN2 / (EW / 4);
+    constexpr int kCols = BNT / (EW / 4);
     const int cb = ((warp - 2) / 4) * kCols;
     int lt = 0;
     for (int t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++lt) {
@@ -888,7 +897,7 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
 #pragma unroll 1
       for (int c0 = cb; c0 < cb + kCols; c0 += 32) {
         uint32_t r[32];
-        tmem_ld32(tmem + (uint32_t)(buf * BN2) + ((uint32_t)(qd * 32) << 16) + (uint32_t)c0, r);
+        tmem_ld32(tmem + (uint32_t)(buf * BNT) + ((uint32_t)(qd * 32) << 16) + (uint32_t)c0, r);
         epi_chunk<MODE>(d.args, row, n0 + c0, r, lane);
       }
       tc_fence_before();
@@ -898,14 +907,14 @@ __device__ __forceinline__ void gemm_persist_body(const CUtensorMap *pCh, const 
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, kTmemColsP);
+  if (warp == 0) tmem_dealloc(tmem, kTC);
 }
 
-template <int MODE, bool A_MN, bool B_MN, bool PER_A>
+template <int MODE, bool A_MN, bool B_MN, bool PER_A, int BNT = BN2>
 __global__ void __launch_bounds__(threads_persist(kEpiWarpsGroup), 1)
     k_gemm_group_persist(const __grid_constant__ CUtensorMap tmCh, const __grid_constant__ CUtensorMap tmCl,
                          const GemmDisk *__restrict__ disks, int tiles_n, int tiles_m, int ntiles) {
-  gemm_persist_body<MODE, A_MN, B_MN, PER_A, kEpiWarpsGroup>(&tmCh, &tmCl, disks, tiles_n, tiles_m, ntiles);
+  gemm_persist_body<MODE, A_MN, B_MN, PER_A, kEpiWarpsGroup, BNT>(&tmCh, &tmCl, disks, tiles_n, tiles_m, ntiles);
 }
 
 // One product of a lone disk by the persistent kernel: A's maps as kernel parameters, B's
@@ -915,7 +924,7 @@ template <int MODE, bool A_MN, bool B_MN>
 __global__ void __launch_bounds__(threads_persist(kEpiWarpsLone), 1)
     k_gemm_persist(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                    const __grid_constant__ GemmDisk b, int tiles_n, int tiles_m, int ntiles) {
-  gemm_persist_body<MODE, A_MN, B_MN, false, kEpiWarpsLone>(&tmAh, &tmAl, &b, tiles_n, tiles_m, ntiles);
+  gemm_persist_body<MODE, A_MN, B_MN, false, kEpiWarpsLone, BN2>(&tmAh, &tmAl, &b, tiles_n, tiles_m, ntiles);
 }
 
 }  // namespace tc
