@@ -71,7 +71,7 @@ struct MixedState {
   enum HydroKind : int { kHydroWarp = 0, kHydroTile = 1, kHydroPacked = 2 };
   int hydro_kind = kHydroTile;
   // pipeline stages of each gravity product (slots: 0 phi DFT, 1-4 the u passes, 5 inverse
-  // phi DFT; 0 = chosen by K, kPersist = the persistent kernel) and the tuner's record
+  // phi DFT; 0 = chosen by K, kPersist / kPersistWide = the persistent kernel) and the tuner's record
   // (autotune below)
   int ns[6] = {0, 0, 0, 0, 0, 0};
   // FP32 field tiles of the packed hydro kernel: sigma, u, w of both ping-pong buffers, dPhi
@@ -589,8 +589,9 @@ static cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, siz
   return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
-// a product slot's "stages" value that selects the persistent GEMM (tc_gemm.cuh)
-constexpr int kPersist = 8;
+// a product slot's "stages" values that select the persistent GEMM (tc_gemm.cuh), with
+// 128 x 128 or (where N is a multiple of 256) 128 x 256 tiles
+constexpr int kPersist = 8, kPersistWide = 16;
 
 // SMs of the current device (the persistent products' grid)
 static int sm_count() {
@@ -609,6 +610,16 @@ static cudaError_t gemm(const CUtensorMap &Ah, const CUtensorMap &Al, const CUte
   tc::GemmArgs a = base;
   a.M = M; a.N = N; a.K = K;
   if (M % tc::BM || N % tc::BN || K % tc::BK) return cudaErrorInvalidValue;
+  if (ns == kPersistWide) {
+    if (N % 256 == 0) {
+      tc::GemmDisk b;
+      b.hi = Bh; b.lo = Bl; b.args = a;
+      const int tn = N / 256, tm = M / tc::BM, nt = tn * tm, nsm = sm_count();
+      return launch_pdl(tc::k_gemm_persist<MODE, A_MN, B_MN, 256>, dim3(nt < nsm ? nt : nsm),
+                        dim3(tc::threads_persist(tc::kEpiWarpsLone)), tc::smem_persist(256), st, Ah, Al, b, tn, tm, nt);
+    }
+    ns = kPersist;  // N not a multiple of 256: 128 x 128 tiles
+  }
   if (ns == kPersist) {
     // the persistent warp-specialised kernel: one CTA per SM walks 128 x 128 tiles, the
     // epilogue of one tile overlapping the loads and MMAs of the next
@@ -642,6 +653,8 @@ template <int MODE, bool A_MN, bool B_MN>
 static cudaError_t prepare_gemm() {
   cudaError_t e;
   e = smem_attrs((const void *)tc::k_gemm_persist<MODE, A_MN, B_MN>, tc::kSmemP);
+  if (e != cudaSuccess) return e;
+  e = smem_attrs((const void *)tc::k_gemm_persist<MODE, A_MN, B_MN, 256>, tc::smem_persist(256));
   if (e != cudaSuccess) return e;
   e = smem_attrs((const void *)tc::k_gemm_split<MODE, A_MN, B_MN, 1>, tc::smem_bytes(1));
   if (e != cudaSuccess) return e;
@@ -1075,14 +1088,16 @@ int dg_handle::mixed_autotune() {
   // the warp form is the only one for odd or narrow grids; a user's choice stands
   const bool hydro_fixed = (hk && *hk) || X.hydro_kind == MixedState::kHydroWarp;
   // DISKGPU_STAGES=s0,s1,s2,s3,s4,s5 fixes the pipeline depth of every gravity product
-  // (0 = chosen by K, else 1, 2 or 4; 8 = the persistent kernel) and skips their tuning
+  // (0 = chosen by K, else 1, 2 or 4; 8 = the persistent kernel, 16 = the same with
+  // 128 x 256 tiles) and skips their tuning
   bool stages_fixed = false;
   if (const char *sv = getenv("DISKGPU_STAGES")) {
     int v[6], n = sscanf(sv, "%d,%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]);
     if (n != 6) return fail(DG_ERR_INVALID, "autotune", "DISKGPU_STAGES wants six comma-separated depths");
     for (int k = 0; k < 6; ++k) {
-      if (v[k] != 0 && v[k] != 1 && v[k] != 2 && v[k] != 4 && v[k] != kPersist)
-        return fail(DG_ERR_INVALID, "autotune", "DISKGPU_STAGES: a depth is 0, 1, 2, 4 or 8 (persistent)");
+      if (v[k] != 0 && v[k] != 1 && v[k] != 2 && v[k] != 4 && v[k] != kPersist && v[k] != kPersistWide)
+        return fail(DG_ERR_INVALID, "autotune",
+                    "DISKGPU_STAGES: a depth is 0, 1, 2, 4, 8 (persistent) or 16 (persistent, 128 x 256 tiles)");
       X.ns[k] = v[k];
     }
     stages_fixed = true;
@@ -1147,7 +1162,7 @@ int dg_handle::mixed_autotune() {
       const float t0 = tbest;
       for (int sl : slots) {
         int keep = X.ns[sl];
-        for (int cand : {1, 2, 4, kPersist}) {
+        for (int cand : {1, 2, 4, kPersist, kPersistWide}) {
           X.ns[sl] = cand;
           float t;
           if ((e = time_us(grav, &t)) != cudaSuccess) break;

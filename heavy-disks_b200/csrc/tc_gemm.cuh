@@ -920,11 +920,11 @@ __global__ void __launch_bounds__(threads_persist(kEpiWarpsGroup), 1)
 // One product of a lone disk by the persistent kernel: A's maps as kernel parameters, B's
 // maps and the epilogue arguments as one by-value entry (a "group" of one disk whose
 // tensor maps TMA reads from the parameter space).
-template <int MODE, bool A_MN, bool B_MN>
+template <int MODE, bool A_MN, bool B_MN, int BNT = BN2>
 __global__ void __launch_bounds__(threads_persist(kEpiWarpsLone), 1)
     k_gemm_persist(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                    const __grid_constant__ GemmDisk b, int tiles_n, int tiles_m, int ntiles) {
-  gemm_persist_body<MODE, A_MN, B_MN, false, kEpiWarpsLone, BN2>(&tmAh, &tmAl, &b, tiles_n, tiles_m, ntiles);
+  gemm_persist_body<MODE, A_MN, B_MN, false, kEpiWarpsLone, BNT>(&tmAh, &tmAl, &b, tiles_n, tiles_m, ntiles);
 }
 
 }  // namespace tc

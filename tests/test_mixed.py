@@ -53,23 +53,25 @@ def test_tensor_core_potential_vs_fp64(Nu, Nphi):
 @pytest.mark.parametrize("Nu,Nphi", [(256, 256), (512, 384), (2048, 128), (4096, 4096)])
 def test_persistent_products_match_tile_products(Nu, Nphi, monkeypatch):
     """Every gravity product on the persistent warp-specialised kernel (DISKGPU_STAGES=8 in
-    every slot; products whose N is not a multiple of 128 stay on the tile kernel) against
+    every slot, and 16: its 128 x 256 tiles where N is a multiple of 256; products whose N
+    is not a multiple of 128 stay on the tile kernel) against
     the tile kernel (stages by K): the same contractions in the same K order, so the
     potentials agree to FP32 round-off, and both meet the FP64 potential to 2e-4.  The grids
     reach the dense products, the four-pass factored u convolution and the four-step phi
     transforms (whose first forward and last inverse passes load blocked operands)."""
     Sig = _field(Nu, Nphi)
     out = {}
-    for stages in ("0,0,0,0,0,0", "8,8,8,8,8,8"):
+    for stages in ("0,0,0,0,0,0", "8,8,8,8,8,8", "16,16,16,16,16,16"):
         monkeypatch.setenv("DISKGPU_STAGES", stages)
         with D.Disk(Nu, Nphi, eps=0.01, precision="mixed") as d:
             d.init_standard()  # applies the fixed stages (the tuner runs on the first state)
             assert "gravity stages fixed " + stages.replace(",", " ") in d.tuning()
             out[stages] = d.potential(Sig)
     ref = O.Kalnajs(Nu, Nphi, eps=0.01).potential(Sig)
-    tile, pers = out["0,0,0,0,0,0"], out["8,8,8,8,8,8"]
-    assert rel_err(pers, ref) < 2e-4
-    assert rel_err(pers, tile) < 1e-6, rel_err(pers, tile)
+    tile = out["0,0,0,0,0,0"]
+    for pers in (out["8,8,8,8,8,8"], out["16,16,16,16,16,16"]):
+        assert rel_err(pers, ref) < 2e-4
+        assert rel_err(pers, tile) < 1e-6, rel_err(pers, tile)
 
 
 def test_state_roundtrip_mixed():
